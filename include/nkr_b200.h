@@ -1,0 +1,204 @@
+/*
+ * nkr_b200.h -- C ABI of the B200 (sm_100a) Groth16 prove backend for BN254.
+ *
+ * This is the drop-in boundary for NKR-ZKP's `groth16-prove --backend b200`.
+ * Every entry point takes plain pointers and sizes; device state lives behind
+ * opaque handles.  Each declaration names the reference interface it replaces
+ * (paths inside the reference project, file:line).
+ *
+ * Byte layouts are the reference's in-memory libff layouts (x86-64):
+ *   Fr / Fq element   32 B: 4 x u64 little-endian, Montgomery form (R = 2^256)
+ *   G1 Jacobian       96 B: {X, Y, Z} Fq, infinity <=> Z = 0      (libff alt_bn128_G1)
+ *   G2 Jacobian      192 B: {X, Y, Z} Fq2, Fq2 = {c0, c1}           (libff alt_bn128_G2)
+ *   CSR matrix        row_ptr u32[rows + 1], col_idx u32[nnz], values Fr[nnz]
+ *                     (protocols/groth16/common/include/r1cs/spmat.hpp:206-215)
+ * Points returned by this library are affine-normalised in that same Jacobian
+ * layout: Z = 1 (Montgomery), or (0, 1, 0) for infinity, exactly what libff's
+ * to_affine_coordinates() produces (libff alt_bn128_g1.cpp to_affine_coordinates).
+ *
+ * Errors: every call returns NKR_B200_OK (0) or a nonzero status; the message
+ * is available from nkr_b200_last_error() on the same thread.  The library
+ * never calls exit() (the reference CUDA path does: operators/cuda/include/
+ * utils/cuda_check.cuh:6-12).  There is no CPU fallback: without a usable
+ * sm_100 device every compute entry point fails with NKR_B200_ENODEV.
+ */
+#ifndef NKR_B200_H
+#define NKR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NKR_B200_OK = 0,
+    NKR_B200_EINVAL = 1,   /* bad argument / shape / size */
+    NKR_B200_ECUDA = 2,    /* CUDA runtime error */
+    NKR_B200_ENOMEM = 3,   /* device memory admission refused */
+    NKR_B200_ENODEV = 4,   /* no usable sm_100 device */
+    NKR_B200_ETIMEOUT = 5, /* bounded device wait expired */
+    NKR_B200_EBUSY = 6     /* server queue full / handle in use */
+};
+
+typedef struct nkr_b200_ctx nkr_b200_ctx;   /* one GPU: streams, scratch arena */
+typedef struct nkr_b200_key nkr_b200_key;   /* a prepared (circuit, proving key) */
+typedef struct nkr_b200_msm_bases nkr_b200_msm_bases; /* resident MSM bases */
+
+/* Circuit in the reference's CSR layout: matrices A, B, C share the shape
+ * rows x cols (protocols/groth16/common/include/groth16/types.hpp:17-27). */
+typedef struct {
+    uint64_t rows;          /* constraints, a power of two >= 2 */
+    uint64_t cols;          /* variables incl. the constant-one column */
+    uint64_t public_inputs; /* number of public inputs (columns 1..public_inputs) */
+    const uint32_t *row_ptr[3];
+    const uint32_t *col_idx[3];
+    const void *values[3]; /* Fr[nnz] Montgomery */
+} nkr_b200_circuit;
+
+/* Proving key queries in libff Jacobian layout, as BinaryArchive stores them
+ * (types.hpp:29-40, io.cpp:54-61).  Points need not be normalised. */
+typedef struct {
+    const void *a_query;    /* G1[cols] */
+    const void *b_g1_query; /* G1[cols] */
+    const void *b_g2_query; /* G2[cols] */
+    const void *l_query;    /* G1[cols] */
+    const void *h_query;    /* G1[rows] */
+    const void *alpha_g1, *beta_g1, *delta_g1; /* G1 */
+    const void *beta_g2, *delta_g2;            /* G2 */
+} nkr_b200_proving_key;
+
+/* RawProof (types.hpp:47-53), affine-normalised libff Jacobian layout */
+typedef struct {
+    uint8_t ar[96], bs1[96], zk[96], qz[96];
+    uint8_t bs2[192];
+} nkr_b200_raw_proof;
+
+/* Proof (types.hpp:55-59) */
+typedef struct {
+    uint8_t a[96];
+    uint8_t b[192];
+    uint8_t c[96];
+} nkr_b200_proof;
+
+/* Per-stage device times of the last prove on a key, milliseconds (CUDA events):
+ * the reference's profile labels groth16.cuda.prove.{r1cs_matrix_vector,
+ * quotient_polynomial, witness_msms, quotient_msm} (groth16_backend.cu:249-274). */
+typedef struct {
+    float spmv_ms, quotient_ms, witness_msms_ms, quotient_msm_ms, total_ms;
+} nkr_b200_stage_times;
+
+/* ---- context -------------------------------------------------------------- */
+
+/* Replaces make_cuda_backend() (backends/cuda/src/groth16_backend.cu:284,
+ * registry common/src/backend_registry.cpp:18-27).  device = CUDA ordinal. */
+int nkr_b200_open(int device, nkr_b200_ctx **out);
+void nkr_b200_close(nkr_b200_ctx *ctx);
+const char *nkr_b200_last_error(void);
+/* "b200" -- Backend::name() (common/include/groth16/backend.hpp:14) */
+const char *nkr_b200_backend_name(void);
+
+/* ---- prove path ----------------------------------------------------------- */
+
+/* Replaces Backend::prepare (backend.hpp:20; CUDA: groth16_backend.cu:214-240):
+ * uploads CSR A/B/C, batch-normalises the PK to affine, builds twiddle tables and
+ * the per-window MSM base copies; all stay resident until nkr_b200_key_free. */
+int nkr_b200_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *circuit,
+                     const nkr_b200_proving_key *pk, nkr_b200_key **out);
+void nkr_b200_key_free(nkr_b200_key *key);
+/* device bytes the key holds */
+uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key);
+
+/* Replaces Backend::prove (backend.hpp:24-28; CPU backends/cpu/src/backend.cpp:156-201,
+ * CUDA groth16_backend.cu:242-279).  witness: Fr[cols] host memory. */
+int nkr_b200_prove(nkr_b200_key *key, const void *witness, uint64_t n,
+                   nkr_b200_raw_proof *out);
+
+/* Replaces blind_proof (common/src/protocol.cpp:85-94) with caller-given r, s
+ * (Fr Montgomery, 32 B each); the reference draws them unseeded (:87-88). */
+int nkr_b200_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r,
+                   const void *s, nkr_b200_proof *out);
+
+/* Intermediates of the last prove on this key, copied to host (for parity
+ * checks): az, bz, cz (Fr[rows]) and H (Fr[rows]); any pointer may be NULL. */
+int nkr_b200_key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h);
+int nkr_b200_key_stage_times(const nkr_b200_key *key, nkr_b200_stage_times *out);
+
+/* Batched prove: count proofs over possibly different keys in one call; the
+ * per-proof stages are issued across streams and replayed from captured CUDA
+ * graphs.  witnesses[i] has keys[i]'s cols elements. */
+int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                         nkr_b200_raw_proof *out);
+
+/* ---- operator-level entry points (operators/cuda/include/nkr/operators/cuda.hpp) */
+
+/* libfqfft radix-2 domain ops on n = 2^k Fr values (host buffer, in place):
+ * op 0 FFT, 1 iFFT, 2 cosetFFT(g = 5), 3 icosetFFT(g = 5), 4 divide_by_Z_on_coset.
+ * Replaces NTTContext::{ntt,intt,coset_ntt,coset_intt} (ntt/ntt.cuh:110-185) and
+ * libfqfft basic_radix2_domain.tcc:40-112. */
+int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n);
+
+/* CSR SpMV over Fr: y = M z (host buffers).  Replaces
+ * sparse_matrix_vector_multiplication (backends/cuda/include/spmvm/spmvm.cuh:12-30). */
+int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_t *row_ptr,
+                  const uint32_t *col_idx, const void *values, const void *z, void *y);
+
+/* Variable-base MSM, bases in libff Jacobian layout (need not be normalised),
+ * scalars Fr Montgomery, result affine-normalised.  Replaces MSMContext::msm
+ * (msm/msm.cuh:82-122) and libff multi_exp BDLO12 (multiexp.tcc:165-282). */
+int nkr_b200_msm_g1(nkr_b200_ctx *ctx, const void *bases, const void *scalars, uint64_t n,
+                    void *out);
+int nkr_b200_msm_g2(nkr_b200_ctx *ctx, const void *bases, const void *scalars, uint64_t n,
+                    void *out);
+
+/* Resident-bases MSM (the prove path's form): bases uploaded and expanded once
+ * into per-window copies, then any number of MSMs with new scalars. */
+int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, uint64_t n,
+                              nkr_b200_msm_bases **out);
+int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t n, void *out,
+                           float *device_ms);
+void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b);
+
+/* ---- field / group primitives (tests and microbenchmarks) ------------------ */
+
+/* Elementwise field op over n pairs (host buffers): field 0 Fr, 1 Fq, 2 Fq2;
+ * op 0 mul, 1 add, 2 sub, 3 sqr, 4 inverse, 5 to_mont, 6 from_mont. */
+int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const void *b,
+                      void *out, uint64_t n);
+/* Elementwise group op: group 1 G1, 2 G2; inputs affine-normalised Jacobian layout.
+ * op 0 add, 1 double (b ignored), 2 scalar multiple by Fr b (Montgomery). */
+int nkr_b200_group_op(nkr_b200_ctx *ctx, int group, int op, const void *a, const void *b,
+                      void *out, uint64_t n);
+/* Throughput microbenchmark of the Montgomery product: field 0 Fr, 1 Fq.
+ * Returns products per second and 32-bit IMAD-class instructions per product. */
+int nkr_b200_bench_mul(nkr_b200_ctx *ctx, int field, double *muls_per_s, double *ms);
+
+/* ---- seeded circuit + witness generators --------------------------------- */
+
+typedef struct nkr_b200_r1cs nkr_b200_r1cs;
+
+/* Builds one of the reference's benchmark circuits with a satisfying witness,
+ * entry for entry as groth16-gen does (protocols/groth16/app/gen.cpp:42-197,
+ * r1cs/r1cs.hpp:64-98), from a seed instead of random_device.
+ * kind: "matmul" (param = size), "poseidon" (param = hash count),
+ * "sql-aggregate" (param = rows, a power of two), "fibonacci" (param = steps).
+ * density: 0 full, 1 hybrid (50%), 2 sparse (10%) (common/include/density.hpp). */
+int nkr_b200_r1cs_generate(const char *kind, uint64_t param, int density, uint64_t seed,
+                           nkr_b200_r1cs **out);
+/* sizes[8] = rows, cols, public_inputs, constraints, variables, nnz A, nnz B, nnz C */
+int nkr_b200_r1cs_info(const nkr_b200_r1cs *r, uint64_t *sizes);
+/* Points a circuit view (and the witness, Fr[cols]) at the generator's arrays;
+ * valid until nkr_b200_r1cs_free. */
+int nkr_b200_r1cs_view(const nkr_b200_r1cs *r, nkr_b200_circuit *view, const void **witness);
+void nkr_b200_r1cs_free(nkr_b200_r1cs *r);
+/* Poseidon hash2 over Fr (Montgomery) -- common/include/crypto/poseidon.hpp:114-119 */
+int nkr_b200_poseidon_hash2(const void *left, const void *right, void *out);
+/* The 195 round constants and 3x3 MDS (Montgomery) -- crypto/poseidon_constants.inc */
+int nkr_b200_poseidon_parameters(void *round_constants, void *mds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NKR_B200_H */

@@ -1,0 +1,404 @@
+// extern "C" surface of libnkr_b200.so (declarations and reference mapping in
+// include/nkr_b200.h).  Every entry point converts failures to a status code
+// plus a thread-local message; nothing here exits the process.
+#include <cstdarg>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "msm.cuh"
+#include "ntt.cuh"
+#include "ops.cuh"
+#include "prover.cuh"
+#include "scan.cuh"
+#include "spmv.cuh"
+
+namespace nkr {
+
+namespace {
+thread_local char g_err[1024] = "";
+std::mutex g_table_mu;
+std::map<std::pair<int, int>, std::unique_ptr<NttTables>> g_tables; // (device, logn)
+} // namespace
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+const char *get_error() { return g_err; }
+
+int device_alloc(void **p, size_t bytes, const char *what)
+{
+    size_t free_b = 0, total_b = 0;
+    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) {
+        set_error("cudaMemGetInfo: %s", cudaGetErrorString(e));
+        return NKR_B200_ECUDA;
+    }
+    // keep 512 MiB of headroom for the runtime and other tenants of the GPU
+    const size_t reserve = size_t(512) << 20;
+    if (bytes + reserve > free_b) {
+        set_error("device memory admission refused for %s: need %zu B, %zu B free", what, bytes,
+                  free_b);
+        return NKR_B200_ENOMEM;
+    }
+    e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+        return NKR_B200_ENOMEM;
+    }
+    return NKR_B200_OK;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_block_totals(uint32_t *totals, uint32_t nb)
+{
+    const uint32_t base = threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = base + i < nb ? totals[base + i] : 0;
+        s += v[i];
+    }
+    uint32_t total;
+    uint32_t run = block_excl_scan(s, &total);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < nb) totals[base + i] = run;
+        run += v[i];
+    }
+}
+
+int get_tables(nkr_b200_ctx *ctx, int logn, const NttTables **out)
+{
+    std::lock_guard<std::mutex> g(g_table_mu);
+    auto &slot = g_tables[{ctx->device, logn}];
+    if (!slot) {
+        auto t = std::make_unique<NttTables>();
+        NKR_TRY(ntt_tables_build(*t, logn, ctx->stream));
+        slot = std::move(t);
+    }
+    *out = slot.get();
+    return NKR_B200_OK;
+}
+
+int key_prepare(nkr_b200_ctx *, const nkr_b200_circuit *, const nkr_b200_proving_key *,
+                nkr_b200_key **);
+int key_prove(nkr_b200_key *, const void *, uint64_t, nkr_b200_raw_proof *);
+int key_blind(nkr_b200_key *, const nkr_b200_raw_proof *, const void *, const void *,
+              nkr_b200_proof *);
+int key_intermediates(nkr_b200_key *, void *, void *, void *, void *);
+int key_prove_batch(nkr_b200_key *const *, const void *const *, int, nkr_b200_raw_proof *);
+
+int ctx_check(nkr_b200_ctx *ctx)
+{
+    NKR_REQUIRE(ctx != nullptr, "null context");
+    NKR_CUDA(cudaSetDevice(ctx->device));
+    return NKR_B200_OK;
+}
+
+} // namespace nkr
+
+struct nkr_b200_msm_bases {
+    nkr_b200_ctx *ctx;
+    nkr::MsmBases bases;
+    nkr::MsmScratch scratch;
+    nkr::DevBuf scalars;
+};
+
+using namespace nkr;
+
+extern "C" {
+
+const char *nkr_b200_last_error(void) { return get_error(); }
+const char *nkr_b200_backend_name(void) { return "b200"; }
+
+int nkr_b200_open(int device, nkr_b200_ctx **out)
+{
+    NKR_REQUIRE(out != nullptr, "null output handle");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available (%s)", cudaGetErrorString(e));
+        return NKR_B200_ENODEV;
+    }
+    NKR_REQUIRE(device >= 0 && device < count, "device %d out of range (%d devices)", device, count);
+    cudaDeviceProp prop{};
+    NKR_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("device %d is sm_%d%d; this library is built for sm_100a only", device,
+                  prop.major, prop.minor);
+        return NKR_B200_ENODEV;
+    }
+    NKR_CUDA(cudaSetDevice(device));
+    auto *ctx = new nkr_b200_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        set_error("stream creation failed");
+        return NKR_B200_ECUDA;
+    }
+    *out = ctx;
+    return NKR_B200_OK;
+}
+
+void nkr_b200_close(nkr_b200_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    {
+        std::lock_guard<std::mutex> g(g_table_mu);
+        for (auto it = g_tables.begin(); it != g_tables.end();)
+            if (it->first.first == ctx->device)
+                it = g_tables.erase(it);
+            else
+                ++it;
+    }
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int nkr_b200_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *circuit,
+                     const nkr_b200_proving_key *pk, nkr_b200_key **out)
+{
+    NKR_TRY(ctx_check(ctx));
+    return key_prepare(ctx, circuit, pk, out);
+}
+
+int nkr_b200_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_proof *out)
+{
+    return key_prove(key, witness, n, out);
+}
+
+int nkr_b200_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r, const void *s,
+                   nkr_b200_proof *out)
+{
+    return key_blind(key, raw, r, s, out);
+}
+
+int nkr_b200_key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
+{
+    return key_intermediates(key, az, bz, cz, h);
+}
+
+int nkr_b200_key_stage_times(const nkr_b200_key *key, nkr_b200_stage_times *out)
+{
+    NKR_REQUIRE(key && out, "null argument");
+    NKR_REQUIRE(key->have_times, "no timed prove on this key yet");
+    *out = key->times;
+    return NKR_B200_OK;
+}
+
+int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                         nkr_b200_raw_proof *out)
+{
+    return key_prove_batch(keys, witnesses, count, out);
+}
+
+int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(data != nullptr, "null data");
+    NKR_REQUIRE(op >= 0 && op <= 4, "ntt op %d unknown", op);
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT size %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)n);
+    const NttTables *T;
+    NKR_TRY(get_tables(ctx, logn, &T));
+    cudaStream_t st = ctx->stream;
+    DevBuf a, b;
+    NKR_TRY(a.alloc(n * 32, "ntt data"));
+    NKR_TRY(b.alloc(n * 32, "ntt scratch"));
+    NKR_CUDA(cudaMemcpyAsync(a.p, data, n * 32, cudaMemcpyHostToDevice, st));
+    const Fr *c = T->consts.as<Fr>();
+    Fr *pa = a.as<Fr>(), *pb = b.as<Fr>();
+    Fr *res = pb;
+    switch (op) {
+    case 0: // FFT
+        NKR_TRY(ntt_dif(*T, pa, false, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, nullptr, st));
+        break;
+    case 1: // iFFT
+        NKR_TRY(ntt_dif(*T, pa, true, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, c + kConstNinv, st));
+        break;
+    case 2: // cosetFFT
+        NKR_TRY(ntt_dif(*T, pa, false, T->gpow.as<Fr>(), nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, nullptr, st));
+        break;
+    case 3: // icosetFFT
+        NKR_TRY(ntt_dif(*T, pa, true, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, T->t2.as<Fr>(), nullptr, st));
+        break;
+    case 4: // divide_by_Z_on_coset
+        NKR_TRY(fr_scale_const(pa, n, c + kConstZinv, st));
+        res = pa;
+        break;
+    }
+    NKR_CUDA(cudaMemcpyAsync(data, res, n * 32, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_t *row_ptr,
+                  const uint32_t *col_idx, const void *values, const void *z, void *y)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(z && y, "null vector");
+    cudaStream_t st = ctx->stream;
+    CsrDevice m;
+    NKR_TRY(csr_upload(m, rows, cols, row_ptr, col_idx, values, st));
+    DevBuf dz, dy;
+    NKR_TRY(dz.alloc(std::max<uint64_t>(cols, 1) * 32, "spmv z"));
+    NKR_TRY(dy.alloc(rows * 32, "spmv y"));
+    NKR_CUDA(cudaMemcpyAsync(dz.p, z, cols * 32, cudaMemcpyHostToDevice, st));
+    const CsrDevice *mats[1] = {&m};
+    Fr *ys[1] = {dy.as<Fr>()};
+    NKR_TRY(spmv_multi(mats, 1, dz.as<Fr>(), ys, st));
+    NKR_CUDA(cudaMemcpyAsync(y, dy.p, rows * 32, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+static int msm_plain(nkr_b200_ctx *ctx, int group, const void *bases, const void *scalars,
+                     uint64_t n, void *out)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(out && (n == 0 || (bases && scalars)), "null argument");
+    cudaStream_t st = ctx->stream;
+    MsmBases b;
+    NKR_TRY(msm_bases_build(b, group, bases, false, n, false, 0, false, st));
+    MsmScratch s;
+    NKR_TRY(msm_scratch_alloc(s, group, b.shape));
+    DevBuf ds;
+    NKR_TRY(ds.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
+    if (n) NKR_CUDA(cudaMemcpyAsync(ds.p, scalars, n * 32, cudaMemcpyHostToDevice, st));
+    NKR_TRY(msm_run(b, s, ds.p, s.result.p, st));
+    NKR_CUDA(cudaMemcpyAsync(out, s.result.p, group == 1 ? 96 : 192, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+int nkr_b200_msm_g1(nkr_b200_ctx *ctx, const void *bases, const void *scalars, uint64_t n, void *out)
+{
+    return msm_plain(ctx, 1, bases, scalars, n, out);
+}
+
+int nkr_b200_msm_g2(nkr_b200_ctx *ctx, const void *bases, const void *scalars, uint64_t n, void *out)
+{
+    return msm_plain(ctx, 2, bases, scalars, n, out);
+}
+
+int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, uint64_t n,
+                              nkr_b200_msm_bases **out)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(out && (n == 0 || bases), "null argument");
+    auto h = std::make_unique<nkr_b200_msm_bases>();
+    h->ctx = ctx;
+    NKR_TRY(msm_bases_build(h->bases, group, bases, false, n, true, 0, false, ctx->stream));
+    NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
+    NKR_TRY(h->scalars.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
+    *out = h.release();
+    return NKR_B200_OK;
+}
+
+int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t n, void *out,
+                           float *device_ms)
+{
+    NKR_REQUIRE(b && out, "null argument");
+    NKR_REQUIRE(n == b->bases.shape.n, "scalar count %llu does not match the %llu bases",
+                (unsigned long long)n, (unsigned long long)b->bases.shape.n);
+    NKR_TRY(ctx_check(b->ctx));
+    cudaStream_t st = b->ctx->stream;
+    cudaMemoryType mt = cudaMemoryTypeUnregistered;
+    {
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, scalars) == cudaSuccess)
+            mt = attr.type;
+        else
+            cudaGetLastError();
+    }
+    const void *src = scalars;
+    if (mt != cudaMemoryTypeDevice) {
+        if (n) NKR_CUDA(cudaMemcpyAsync(b->scalars.p, scalars, n * 32, cudaMemcpyHostToDevice, st));
+        src = b->scalars.p;
+    }
+    cudaEvent_t e0, e1;
+    NKR_CUDA(cudaEventCreate(&e0));
+    NKR_CUDA(cudaEventCreate(&e1));
+    NKR_CUDA(cudaEventRecord(e0, st));
+    const int s = msm_run(b->bases, b->scratch, src, b->scratch.result.p, st);
+    NKR_CUDA(cudaEventRecord(e1, st));
+    NKR_CUDA(cudaMemcpyAsync(out, b->scratch.result.p, b->bases.group == 1 ? 96 : 192,
+                             cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    if (device_ms) cudaEventElapsedTime(device_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return s;
+}
+
+void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+}
+
+int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const void *b, void *out,
+                      uint64_t n)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(a && out, "null argument");
+    const size_t esz = field == 2 ? 64 : 32;
+    cudaStream_t st = ctx->stream;
+    DevBuf da, db, dout;
+    NKR_TRY(da.alloc(std::max<uint64_t>(n, 1) * esz, "field op a"));
+    NKR_TRY(db.alloc(std::max<uint64_t>(n, 1) * esz, "field op b"));
+    NKR_TRY(dout.alloc(std::max<uint64_t>(n, 1) * esz, "field op out"));
+    NKR_CUDA(cudaMemcpyAsync(da.p, a, n * esz, cudaMemcpyHostToDevice, st));
+    if (b) NKR_CUDA(cudaMemcpyAsync(db.p, b, n * esz, cudaMemcpyHostToDevice, st));
+    NKR_TRY(field_op_device(field, op, da.p, b ? db.p : nullptr, dout.p, n, st));
+    NKR_CUDA(cudaMemcpyAsync(out, dout.p, n * esz, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+int nkr_b200_group_op(nkr_b200_ctx *ctx, int group, int op, const void *a, const void *b, void *out,
+                      uint64_t n)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(a && out && (op == 1 || b), "null argument");
+    const size_t psz = group == 1 ? 96 : 192;
+    const size_t bsz = op == 2 ? 32 : psz;
+    cudaStream_t st = ctx->stream;
+    DevBuf da, db, dout;
+    NKR_TRY(da.alloc(std::max<uint64_t>(n, 1) * psz, "group op a"));
+    NKR_TRY(db.alloc(std::max<uint64_t>(n, 1) * bsz, "group op b"));
+    NKR_TRY(dout.alloc(std::max<uint64_t>(n, 1) * psz, "group op out"));
+    NKR_CUDA(cudaMemcpyAsync(da.p, a, n * psz, cudaMemcpyHostToDevice, st));
+    if (b) NKR_CUDA(cudaMemcpyAsync(db.p, b, n * bsz, cudaMemcpyHostToDevice, st));
+    NKR_TRY(group_op_device(group, op, da.p, db.p, dout.p, n, st));
+    NKR_CUDA(cudaMemcpyAsync(out, dout.p, n * psz, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+int nkr_b200_bench_mul(nkr_b200_ctx *ctx, int field, double *muls_per_s, double *ms)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(muls_per_s && ms, "null argument");
+    return bench_mul_device(field, ctx->sm_count, muls_per_s, ms, ctx->stream);
+}
+
+} // extern "C"

@@ -1,0 +1,355 @@
+// BN254 base field Fq and scalar field Fr on sm_100a.
+//
+// Representation: 8 x 32-bit little-endian limbs in Montgomery form
+// (R = 2^256), always fully reduced (< modulus).  The byte image is identical
+// to libff's Fp_model<4, modulus>::mont_repr on x86-64, so device buffers are
+// bit-for-bit the reference's host vectors (reference: libff
+// algebra/fields/fp.hpp:40-42, CUDA mont_t layout operators/cuda/include/fields/
+// mont_t.cuh:45).
+//
+// Multiplication is CIOS Montgomery: per limb of b, one carry chain adds the
+// low halves of a*b_i, one adds the high halves, then the reduction by
+// m = t0 * (-p^-1) repeats the pair of chains with the modulus as immediates.
+// Because p < 2^254, the running value stays below 2p and 9 words suffice.
+#pragma once
+
+#include <cstdint>
+
+namespace nkr {
+
+struct FqParams {
+    static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du,
+                              P3 = 0x97816a91u, P4 = 0x8181585du, P5 = 0xb85045b6u,
+                              P6 = 0xe131a029u, P7 = 0x30644e72u;
+    static constexpr uint32_t INV = 0xe4866389u; // -p^-1 mod 2^32
+    static constexpr uint32_t O0 = 0xc58f0d9du, O1 = 0xd35d438du, O2 = 0xf5c70b3du, O3 = 0x0a78eb28u, O4 = 0x7879462cu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+    static constexpr uint32_t Q0 = 0x538afa89u, Q1 = 0xf32cfc5bu, Q2 = 0xd44501fbu, Q3 = 0xb5e71911u, Q4 = 0x0a417ff6u, Q5 = 0x47ab1effu, Q6 = 0xcab8351fu, Q7 = 0x06d89f71u;
+};
+
+struct FrParams {
+    static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u,
+                              P3 = 0x2833e848u, P4 = 0x8181585du, P5 = 0xb85045b6u,
+                              P6 = 0xe131a029u, P7 = 0x30644e72u;
+    static constexpr uint32_t INV = 0xefffffffu;
+    static constexpr uint32_t O0 = 0x4ffffffbu, O1 = 0xac96341cu, O2 = 0x9f60cd29u, O3 = 0x36fc7695u, O4 = 0x7879462eu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+    static constexpr uint32_t Q0 = 0xae216da7u, Q1 = 0x1bb8e645u, Q2 = 0xe35c59e3u, Q3 = 0x53fe3ab1u, Q4 = 0x53bb8085u, Q5 = 0x8c49833du, Q6 = 0x7f4e44a5u, Q7 = 0x0216d0b1u;
+};
+
+template <class P>
+struct alignas(32) Fp {
+    uint32_t v[8];
+
+    __device__ __forceinline__ static Fp zero()
+    {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) r.v[i] = 0;
+        return r;
+    }
+    __device__ __forceinline__ static Fp one()
+    {
+        return {{P::O0, P::O1, P::O2, P::O3, P::O4, P::O5, P::O6, P::O7}};
+    }
+    __device__ __forceinline__ static Fp r2()
+    {
+        return {{P::Q0, P::Q1, P::Q2, P::Q3, P::Q4, P::Q5, P::Q6, P::Q7}};
+    }
+    __device__ __forceinline__ bool is_zero() const
+    {
+        uint32_t x = v[0];
+#pragma unroll
+        for (int i = 1; i < 8; ++i) x |= v[i];
+        return x == 0;
+    }
+    __device__ __forceinline__ bool operator==(const Fp &o) const
+    {
+        uint32_t x = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x |= v[i] ^ o.v[i];
+        return x == 0;
+    }
+    __device__ __forceinline__ bool operator!=(const Fp &o) const { return !(*this == o); }
+};
+
+using Fq = Fp<FqParams>;
+using Fr = Fp<FrParams>;
+
+// ---------------------------------------------------------------------------
+// conditional subtraction of the modulus: r = (t >= p) ? t - p : t
+// ---------------------------------------------------------------------------
+template <class P>
+__device__ __forceinline__ void reduce_once(uint32_t *t)
+{
+    uint32_t s0, s1, s2, s3, s4, s5, s6, s7, br;
+    asm("sub.cc.u32  %0, %9,  %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(s0), "=r"(s1), "=r"(s2), "=r"(s3), "=r"(s4), "=r"(s5), "=r"(s6), "=r"(s7),
+          "=r"(br)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]),
+          "r"(t[7]), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5),
+          "n"(P::P6), "n"(P::P7));
+    // br == 0xffffffff when t < p (keep t), 0 when t >= p (take t - p)
+    const bool keep = br != 0;
+    t[0] = keep ? t[0] : s0;
+    t[1] = keep ? t[1] : s1;
+    t[2] = keep ? t[2] : s2;
+    t[3] = keep ? t[3] : s3;
+    t[4] = keep ? t[4] : s4;
+    t[5] = keep ? t[5] : s5;
+    t[6] = keep ? t[6] : s6;
+    t[7] = keep ? t[7] : s7;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> operator+(const Fp<P> &a, const Fp<P> &b)
+{
+    Fp<P> r;
+    asm("add.cc.u32  %0, %8,  %16;\n\t"
+        "addc.cc.u32 %1, %9,  %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+          "=r"(r.v[6]), "=r"(r.v[7])
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]),
+          "r"(a.v[6]), "r"(a.v[7]), "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]),
+          "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    reduce_once<P>(r.v);
+    return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> operator-(const Fp<P> &a, const Fp<P> &b)
+{
+    Fp<P> r;
+    uint32_t br;
+    asm("sub.cc.u32  %0, %9,  %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+          "=r"(r.v[6]), "=r"(r.v[7]), "=r"(br)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]),
+          "r"(a.v[6]), "r"(a.v[7]), "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]),
+          "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    // on borrow add p back (br is an all-ones mask)
+    asm("add.cc.u32  %0, %0, %8;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, %10;\n\t"
+        "addc.cc.u32 %3, %3, %11;\n\t"
+        "addc.cc.u32 %4, %4, %12;\n\t"
+        "addc.cc.u32 %5, %5, %13;\n\t"
+        "addc.cc.u32 %6, %6, %14;\n\t"
+        "addc.u32    %7, %7, %15;"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]),
+          "+r"(r.v[6]), "+r"(r.v[7])
+        : "r"(P::P0 & br), "r"(P::P1 & br), "r"(P::P2 & br), "r"(P::P3 & br), "r"(P::P4 & br),
+          "r"(P::P5 & br), "r"(P::P6 & br), "r"(P::P7 & br));
+    return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> neg(const Fp<P> &a)
+{
+    return Fp<P>::zero() - a;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> dbl(const Fp<P> &a)
+{
+    return a + a;
+}
+
+// One CIOS round: t[0..8] += a * bi; m = t0 * inv; t += m * p; t >>= 32.
+#define NKR_CIOS_ROUND(bi)                                                                     \
+    asm("mad.lo.cc.u32  %0, %9,  %17, %0;\n\t"                                                 \
+        "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                 \
+        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                 \
+        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                 \
+        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                 \
+        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                 \
+        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                 \
+        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                 \
+        "addc.u32       %8, %8, 0;\n\t"                                                        \
+        "mad.hi.cc.u32  %1, %9,  %17, %1;\n\t"                                                 \
+        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                 \
+        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                 \
+        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                 \
+        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                 \
+        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                 \
+        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                 \
+        "madc.hi.u32    %8, %16, %17, %8;"                                                     \
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7),      \
+          "+r"(t8)                                                                             \
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]),        \
+          "r"(a.v[6]), "r"(a.v[7]), "r"(bi));                                                  \
+    {                                                                                          \
+        const uint32_t m = t0 * P::INV;                                                        \
+        asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                              \
+            "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                              \
+            "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                              \
+            "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                              \
+            "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                              \
+            "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                              \
+            "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                              \
+            "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                              \
+            "addc.u32       %8, %8, 0;\n\t"                                                    \
+            "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                              \
+            "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                              \
+            "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                              \
+            "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                              \
+            "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                              \
+            "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                              \
+            "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                              \
+            "madc.hi.u32    %8, %9, %17, %8;"                                                  \
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7),  \
+              "+r"(t8)                                                                         \
+            : "r"(m), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5),  \
+              "n"(P::P6), "n"(P::P7));                                                         \
+    }                                                                                          \
+    t0 = t1;                                                                                   \
+    t1 = t2;                                                                                   \
+    t2 = t3;                                                                                   \
+    t3 = t4;                                                                                   \
+    t4 = t5;                                                                                   \
+    t5 = t6;                                                                                   \
+    t6 = t7;                                                                                   \
+    t7 = t8;                                                                                   \
+    t8 = 0;
+
+template <class P>
+__device__ __forceinline__ Fp<P> operator*(const Fp<P> &a, const Fp<P> &b)
+{
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+    NKR_CIOS_ROUND(b.v[0])
+    NKR_CIOS_ROUND(b.v[1])
+    NKR_CIOS_ROUND(b.v[2])
+    NKR_CIOS_ROUND(b.v[3])
+    NKR_CIOS_ROUND(b.v[4])
+    NKR_CIOS_ROUND(b.v[5])
+    NKR_CIOS_ROUND(b.v[6])
+    NKR_CIOS_ROUND(b.v[7])
+    Fp<P> r;
+    r.v[0] = t0;
+    r.v[1] = t1;
+    r.v[2] = t2;
+    r.v[3] = t3;
+    r.v[4] = t4;
+    r.v[5] = t5;
+    r.v[6] = t6;
+    r.v[7] = t7;
+    (void)t8;
+    reduce_once<P>(r.v);
+    return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> sqr(const Fp<P> &a)
+{
+    return a * a;
+}
+
+// Montgomery -> canonical integer (same limb layout)
+template <class P>
+__device__ __forceinline__ Fp<P> from_mont(const Fp<P> &a)
+{
+    Fp<P> one;
+    one.v[0] = 1;
+#pragma unroll
+    for (int i = 1; i < 8; ++i) one.v[i] = 0;
+    return a * one;
+}
+
+// canonical integer (< p) -> Montgomery
+template <class P>
+__device__ __forceinline__ Fp<P> to_mont(const Fp<P> &a)
+{
+    return a * Fp<P>::r2();
+}
+
+// a^e for a small public exponent given as 8 limbs (left-to-right square-and-multiply)
+template <class P>
+__device__ Fp<P> pow_limbs(const Fp<P> &a, const uint32_t *e)
+{
+    Fp<P> acc = Fp<P>::one();
+    for (int i = 255; i >= 0; --i) {
+        acc = sqr(acc);
+        if ((e[i >> 5] >> (i & 31)) & 1) acc = acc * a;
+    }
+    return acc;
+}
+
+// Fermat inverse: a^(p-2).  0 maps to 0.
+template <class P>
+__device__ Fp<P> inverse(const Fp<P> &a)
+{
+    const uint32_t e[8] = {P::P0 - 2u, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
+    return pow_limbs(a, e);
+}
+
+// ---------------------------------------------------------------------------
+// Fq2 = Fq[u] / (u^2 + 1)  (libff alt_bn128_Fq2, non_residue = -1)
+// ---------------------------------------------------------------------------
+struct alignas(32) Fq2 {
+    Fq c0, c1;
+    __device__ __forceinline__ static Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
+    __device__ __forceinline__ static Fq2 one() { return {Fq::one(), Fq::zero()}; }
+    __device__ __forceinline__ bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+    __device__ __forceinline__ bool operator==(const Fq2 &o) const
+    {
+        return c0 == o.c0 && c1 == o.c1;
+    }
+    __device__ __forceinline__ bool operator!=(const Fq2 &o) const { return !(*this == o); }
+};
+
+__device__ __forceinline__ Fq2 operator+(const Fq2 &a, const Fq2 &b)
+{
+    return {a.c0 + b.c0, a.c1 + b.c1};
+}
+__device__ __forceinline__ Fq2 operator-(const Fq2 &a, const Fq2 &b)
+{
+    return {a.c0 - b.c0, a.c1 - b.c1};
+}
+__device__ __forceinline__ Fq2 neg(const Fq2 &a) { return {neg(a.c0), neg(a.c1)}; }
+__device__ __forceinline__ Fq2 dbl(const Fq2 &a) { return {dbl(a.c0), dbl(a.c1)}; }
+
+// Karatsuba: 3 base-field products
+__device__ __forceinline__ Fq2 operator*(const Fq2 &a, const Fq2 &b)
+{
+    const Fq v0 = a.c0 * b.c0;
+    const Fq v1 = a.c1 * b.c1;
+    const Fq s = (a.c0 + a.c1) * (b.c0 + b.c1);
+    return {v0 - v1, s - v0 - v1};
+}
+
+// (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
+__device__ __forceinline__ Fq2 sqr(const Fq2 &a)
+{
+    const Fq p = (a.c0 + a.c1) * (a.c0 - a.c1);
+    const Fq q = a.c0 * a.c1;
+    return {p, q + q};
+}
+
+__device__ inline Fq2 inverse(const Fq2 &a)
+{
+    const Fq n = sqr(a.c0) + sqr(a.c1);
+    const Fq ni = inverse(n);
+    return {a.c0 * ni, neg(a.c1) * ni};
+}
+
+} // namespace nkr

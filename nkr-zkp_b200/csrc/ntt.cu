@@ -1,0 +1,289 @@
+// Radix-2 NTT kernels and resident tables (see ntt.cuh for the design).
+#include "ntt.cuh"
+
+namespace nkr {
+
+namespace {
+
+// 2^28-th root of unity of Fr in Montgomery form: 5^((r - 1) / 2^28), the root
+// libff uses (alt_bn128_init.cpp:56-61 with multiplicative_generator = 5 and
+// s = 28; field_utils.tcc:38-51 squares it down to smaller domains).
+__device__ __forceinline__ Fr fr_root_2_28()
+{
+    Fr r;
+    const uint32_t v[8] = {0x80d13d9cu, 0x636e7355u, 0x2445ffd6u, 0xa22bf374u,
+                           0x1eb203d8u, 0x56452ac0u, 0x2963f9e7u, 0x1860ef94u};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = v[i];
+    return r;
+}
+
+// multiplicative generator g = 5 (Montgomery), the coset shift of cosetFFT
+__device__ __forceinline__ Fr fr_gen5()
+{
+    Fr r;
+    const uint32_t v[8] = {0x9fffffe6u, 0x1b0d0ef9u, 0xa32a913fu, 0xeaba68a3u,
+                           0xd8dd0689u, 0x47d8eb76u, 0x20f5bbc3u, 0x15d00855u};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = v[i];
+    return r;
+}
+
+__global__ void k_ntt_constants(int logn, Fr *c)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Fr w = fr_root_2_28();
+    for (int i = 28; i > logn; --i) w = sqr(w);
+    Fr nn = Fr::zero();
+    nn.v[0] = uint32_t(1u << logn);
+    nn = to_mont(nn);
+    const Fr g = fr_gen5();
+    Fr gn = g;
+    for (int i = 0; i < logn; ++i) gn = sqr(gn);
+    c[kConstOmega] = w;
+    c[kConstOmegaInv] = inverse(w);
+    c[kConstNinv] = inverse(nn);
+    c[kConstZinv] = inverse(gn - Fr::one());
+    c[kConstG] = g;
+    c[kConstGinv] = inverse(g);
+    c[6] = Fr::one();
+    c[7] = Fr::zero();
+}
+
+// out[i] = base^i, i < m; each thread fills a run of 32 consecutive powers
+constexpr int kPowRun = 32;
+__global__ void k_powers(const Fr *base_ptr, Fr *out, uint64_t m)
+{
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t first = t * kPowRun;
+    if (first >= m) return;
+    const Fr base = *base_ptr;
+    Fr acc = Fr::one();
+    // base^first by square-and-multiply over the bits of first
+    for (int b = 63; b >= 0; --b) {
+        acc = sqr(acc);
+        if ((first >> b) & 1) acc = acc * base;
+    }
+    for (int i = 0; i < kPowRun && first + i < m; ++i) {
+        out[first + i] = acc;
+        acc = acc * base;
+    }
+}
+
+// tw[2^s + k] = pw[k << (logn - 1 - s)]  (w_{2^(s+1)}^k from powers of w_N)
+__global__ void k_stage_twiddles(const Fr *pw, Fr *tw, int logn)
+{
+    const uint64_t n = uint64_t(1) << logn;
+    const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    if (j == 0) {
+        tw[0] = Fr::one();
+        return;
+    }
+    const int s = 63 - __clzll((long long)j);
+    const uint64_t k = j - (uint64_t(1) << s);
+    tw[j] = pw[k << (logn - 1 - s)];
+}
+
+__device__ __forceinline__ uint32_t brev_n(uint32_t j, int logn)
+{
+    return logn == 0 ? 0u : (__brev(j) >> (32 - logn));
+}
+
+// dst[j] = c * src[bitrev(j)]
+__global__ void k_bitrev_scaled(const Fr *src, const Fr *c, Fr *dst, int logn)
+{
+    const uint64_t n = uint64_t(1) << logn;
+    const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    dst[j] = *c * src[brev_n(uint32_t(j), logn)];
+}
+
+template <bool DIF>
+__global__ void __launch_bounds__(512) k_ntt_pass(Fr *data, int s_lo, int t, const Fr *tw,
+                                                   const Fr *pre, const Fr *post,
+                                                   const Fr *post_const)
+{
+    extern __shared__ Fr sm[];
+    const int G = 1 << t;
+    const int half = G >> 1;
+    const uint64_t gid = blockIdx.x;
+    const uint64_t low = gid & ((uint64_t(1) << s_lo) - 1);
+    const uint64_t high = gid >> s_lo;
+    const uint64_t base = low | (high << (s_lo + t));
+
+    for (int m = threadIdx.x; m < G; m += blockDim.x) {
+        const uint64_t j = base + (uint64_t(m) << s_lo);
+        Fr x = data[j];
+        if (pre) x = x * pre[j];
+        sm[m] = x;
+    }
+    __syncthreads();
+    for (int st = 0; st < t; ++st) {
+        const int s = DIF ? (s_lo + t - 1 - st) : (s_lo + st);
+        const int dl = s - s_lo;
+        const int d = 1 << dl;
+        for (int b = threadIdx.x; b < half; b += blockDim.x) {
+            const int m0 = ((b >> dl) << (dl + 1)) | (b & (d - 1));
+            const int m1 = m0 + d;
+            const uint64_t k = (uint64_t(m0 & (d - 1)) << s_lo) | low;
+            const Fr w = tw[(uint64_t(1) << s) + k];
+            const Fr u = sm[m0];
+            const Fr v = sm[m1];
+            if (DIF) {
+                sm[m0] = u + v;
+                sm[m1] = (u - v) * w;
+            } else {
+                const Fr tv = v * w;
+                sm[m0] = u + tv;
+                sm[m1] = u - tv;
+            }
+        }
+        __syncthreads();
+    }
+    for (int m = threadIdx.x; m < G; m += blockDim.x) {
+        const uint64_t j = base + (uint64_t(m) << s_lo);
+        Fr x = sm[m];
+        if (post)
+            x = x * post[j];
+        else if (post_const)
+            x = x * *post_const;
+        data[j] = x;
+    }
+}
+
+__global__ void k_bitrev_permute(const Fr *in, Fr *out, int logn, const Fr *scale,
+                                 const Fr *scale_const)
+{
+    const uint64_t n = uint64_t(1) << logn;
+    const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    Fr x = in[j];
+    if (scale)
+        x = x * scale[j];
+    else if (scale_const)
+        x = x * *scale_const;
+    out[brev_n(uint32_t(j), logn)] = x;
+}
+
+__global__ void k_scale_const(Fr *d, uint64_t n, const Fr *c)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = d[i] * *c;
+}
+
+__global__ void k_quotient(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_t n,
+                           const Fr *zinv)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) h[i] = (a[i] * b[i] - c[i]) * *zinv;
+}
+
+// pass split: at most 10 radix-2 stages per pass, spread evenly
+int pass_plan(int logn, int *ts)
+{
+    const int np = (logn + 9) / 10;
+    for (int i = 0; i < np; ++i) ts[i] = logn / np + (i < logn % np ? 1 : 0);
+    return np;
+}
+
+int run_passes(const NttTables &tb, Fr *data, bool dif, bool inverse, const Fr *pre,
+               const Fr *post, const Fr *post_const, cudaStream_t st)
+{
+    const int logn = tb.logn;
+    int ts[4];
+    const int np = pass_plan(logn, ts);
+    const Fr *tw = inverse ? tb.tw_inv.as<Fr>() : tb.tw_fwd.as<Fr>();
+    int s_lo = dif ? logn : 0;
+    for (int p = 0; p < np; ++p) {
+        const int t = ts[p];
+        if (dif) s_lo -= t;
+        const int G = 1 << t;
+        const unsigned threads = G >= 64 ? unsigned(G / 2) : 32u;
+        const unsigned blocks = unsigned(tb.n >> t);
+        const Fr *pr = p == 0 ? pre : nullptr;
+        const Fr *po = p == np - 1 ? post : nullptr;
+        const Fr *pc = p == np - 1 ? post_const : nullptr;
+        if (dif)
+            k_ntt_pass<true><<<blocks, threads, G * sizeof(Fr), st>>>(data, s_lo, t, tw, pr, po, pc);
+        else
+            k_ntt_pass<false><<<blocks, threads, G * sizeof(Fr), st>>>(data, s_lo, t, tw, pr, po, pc);
+        NKR_CHECK_LAUNCH();
+        if (!dif) s_lo += t;
+    }
+    return NKR_B200_OK;
+}
+
+} // namespace
+
+int ntt_tables_build(NttTables &t, int logn, cudaStream_t st)
+{
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT domain 2^%d outside [2, 2^28]", logn);
+    t.logn = logn;
+    t.n = uint64_t(1) << logn;
+    const size_t bytes = t.n * sizeof(Fr);
+    NKR_TRY(t.consts.alloc(8 * sizeof(Fr), "ntt constants"));
+    NKR_TRY(t.tw_fwd.alloc(bytes, "ntt twiddles"));
+    NKR_TRY(t.tw_inv.alloc(bytes, "ntt inverse twiddles"));
+    NKR_TRY(t.gpow.alloc(bytes, "coset powers"));
+    NKR_TRY(t.t1.alloc(bytes, "coset scale table"));
+    NKR_TRY(t.t2.alloc(bytes, "inverse coset scale table"));
+    DevBuf tmp;
+    NKR_TRY(tmp.alloc(bytes, "ntt table scratch"));
+    Fr *c = t.consts.as<Fr>();
+    k_ntt_constants<<<1, 32, 0, st>>>(logn, c);
+    const unsigned pb = blocks_for((t.n + kPowRun - 1) / kPowRun, 128);
+    const unsigned nb = blocks_for(t.n, 256);
+    // forward stage twiddles from powers of w (tmp holds w^i, i < N/2)
+    k_powers<<<pb, 128, 0, st>>>(c + kConstOmega, tmp.as<Fr>(), t.n / 2);
+    k_stage_twiddles<<<nb, 256, 0, st>>>(tmp.as<Fr>(), t.tw_fwd.as<Fr>(), logn);
+    k_powers<<<pb, 128, 0, st>>>(c + kConstOmegaInv, tmp.as<Fr>(), t.n / 2);
+    k_stage_twiddles<<<nb, 256, 0, st>>>(tmp.as<Fr>(), t.tw_inv.as<Fr>(), logn);
+    // g^i natural, then the bit-reversed scale tables
+    k_powers<<<pb, 128, 0, st>>>(c + kConstG, t.gpow.as<Fr>(), t.n);
+    k_bitrev_scaled<<<nb, 256, 0, st>>>(t.gpow.as<Fr>(), c + kConstNinv, t.t1.as<Fr>(), logn);
+    k_powers<<<pb, 128, 0, st>>>(c + kConstGinv, tmp.as<Fr>(), t.n);
+    k_bitrev_scaled<<<nb, 256, 0, st>>>(tmp.as<Fr>(), c + kConstNinv, t.t2.as<Fr>(), logn);
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+int ntt_dif(const NttTables &t, Fr *data, bool inverse, const Fr *pre, const Fr *post,
+            const Fr *post_const, cudaStream_t st)
+{
+    return run_passes(t, data, true, inverse, pre, post, post_const, st);
+}
+
+int ntt_dit(const NttTables &t, Fr *data, bool inverse, const Fr *pre, const Fr *post,
+            const Fr *post_const, cudaStream_t st)
+{
+    return run_passes(t, data, false, inverse, pre, post, post_const, st);
+}
+
+int ntt_bitrev_permute(const Fr *in, Fr *out, uint64_t n, const Fr *scale, const Fr *scale_const,
+                       cudaStream_t st)
+{
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 0 && logn <= 31, "bit reversal needs a power-of-two size");
+    k_bitrev_permute<<<blocks_for(n, 256), 256, 0, st>>>(in, out, logn, scale, scale_const);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int fr_scale_const(Fr *data, uint64_t n, const Fr *c, cudaStream_t st)
+{
+    k_scale_const<<<blocks_for(n, 256), 256, 0, st>>>(data, n, c);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int fr_quotient_pointwise(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_t n,
+                          const Fr *zinv, cudaStream_t st)
+{
+    k_quotient<<<blocks_for(n, 256), 256, 0, st>>>(a, b, c, h, n, zinv);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+} // namespace nkr

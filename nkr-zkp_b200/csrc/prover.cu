@@ -1,0 +1,411 @@
+// Groth16 prepare / prove / blind on one B200 (design notes in prover.cuh).
+#include <cstring>
+#include <vector>
+
+#include "prover.cuh"
+
+namespace nkr {
+
+namespace {
+
+constexpr size_t kOutBytes = 4 * 96 + 192; // ar, bs1, zk, qz (G1) + bs2 (G2)
+constexpr size_t kOutOffset[kNumMsm] = {0, 96, 192, 288, 384}; // A, B1, L, H, B2
+
+// ---------------------------------------------------------------------------
+// blinding (protocol.cpp:85-94) with caller-supplied r, s
+// ---------------------------------------------------------------------------
+
+template <class F>
+__device__ __forceinline__ Affine<F> load_libff_affine(const F *p)
+{
+    if (p[2].is_zero()) return Affine<F>::inf();
+    return {p[0], p[1]};
+}
+
+template <class F>
+__device__ __forceinline__ void store_libff(const Xyzz<F> &x, F *out)
+{
+    const Affine<F> a = xyzz_to_affine(x);
+    if (a.is_inf()) {
+        out[0] = F::zero();
+        out[1] = F::one();
+        out[2] = F::zero();
+    } else {
+        out[0] = a.x;
+        out[1] = a.y;
+        out[2] = F::one();
+    }
+}
+
+// pk_const: alpha_g1, beta_g1, delta_g1 (G1Affine) then beta_g2, delta_g2 (G2Affine)
+// raw: libff layout ar, bs1, zk, qz (G1), bs2 (G2); rs: r, s (Montgomery)
+// out: A (G1, 96 B), B (G2, 192 B), C (G1, 96 B) in libff layout
+__global__ void k_blind(const uint8_t *pk_const, const uint8_t *raw, const Fr *rs, uint8_t *out)
+{
+    __shared__ G1Xyzz g1p[6];
+    __shared__ G2Xyzz g2p;
+    const G1Affine *g1c = reinterpret_cast<const G1Affine *>(pk_const);
+    const G2Affine *g2c = reinterpret_cast<const G2Affine *>(pk_const + 3 * sizeof(G1Affine));
+    const Fq *rq = reinterpret_cast<const Fq *>(raw);
+    const G1Affine ar = load_libff_affine(rq + 0), bs1 = load_libff_affine(rq + 3),
+                   zk = load_libff_affine(rq + 6), qz = load_libff_affine(rq + 9);
+    const G2Affine bs2 = load_libff_affine(reinterpret_cast<const Fq2 *>(raw + 384));
+    const Fr r = from_mont(rs[0]), s = from_mont(rs[1]), rsp = from_mont(rs[0] * rs[1]);
+    // independent scalar multiples, one per warp (lane 0) so they run concurrently
+    const int t = (threadIdx.x & 31) ? -1 : int(threadIdx.x >> 5);
+    if (t == 0) g1p[0] = xyzz_mul_canon(g1c[2], r.v);   // r delta1
+    if (t == 1) g1p[1] = xyzz_mul_canon(g1c[0], s.v);   // s alpha1
+    if (t == 2) g1p[2] = xyzz_mul_canon(g1c[1], r.v);   // r beta1
+    if (t == 3) g1p[3] = xyzz_mul_canon(g1c[2], rsp.v); // rs delta1
+    if (t == 4) g1p[4] = xyzz_mul_canon(ar, s.v);       // s ar
+    if (t == 5) g1p[5] = xyzz_mul_canon(bs1, r.v);      // r bs1
+    if (t == 6) g2p = xyzz_mul_canon(g2c[1], s.v);      // s delta2
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    // A = alpha1 + ar + r delta1
+    G1Xyzz A = xyzz_add_affine(xyzz_add_affine(g1p[0], g1c[0]), ar);
+    // B = beta2 + bs2 + s delta2
+    G2Xyzz B = xyzz_add_affine(xyzz_add_affine(g2p, g2c[0]), bs2);
+    // C = qz + zk + s A + r B1 - rs delta1
+    //   = qz + zk + s alpha1 + s ar + r beta1 + r bs1 + rs delta1
+    G1Xyzz C = xyzz_add_affine(xyzz_add_affine(g1p[1], qz), zk);
+    C = xyzz_add(C, g1p[4]);
+    C = xyzz_add(C, g1p[2]);
+    C = xyzz_add(C, g1p[5]);
+    C = xyzz_add(C, g1p[3]);
+    store_libff(A, reinterpret_cast<Fq *>(out));
+    store_libff(B, reinterpret_cast<Fq2 *>(out + 96));
+    store_libff(C, reinterpret_cast<Fq *>(out + 288));
+}
+
+int check_witness_ptr(const void *p, cudaMemoryType *type)
+{
+    cudaPointerAttributes attr{};
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *type = cudaMemoryTypeUnregistered;
+        return NKR_B200_OK;
+    }
+    *type = attr.type;
+    return NKR_B200_OK;
+}
+
+} // namespace
+
+int prove_issue(nkr_b200_key *key, bool timed)
+{
+    cudaStream_t s0 = key->st[kMsmH];
+    const uint64_t rows = key->rows;
+    Fr *z = key->z.as<Fr>();
+    Fr *az = key->az.as<Fr>(), *bz = key->bz.as<Fr>(), *cz = key->cz.as<Fr>(), *h = key->h.as<Fr>();
+    uint8_t *out = key->out.as<uint8_t>();
+    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[0], s0));
+    const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
+    Fr *ys[3] = {az, bz, cz};
+    NKR_TRY(spmv_multi(mats, 3, z, ys, s0));
+    NKR_CUDA(cudaEventRecord(key->ev_z, s0));
+    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[1], s0));
+    // witness MSMs on their own streams, overlapping the H chain
+    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) {
+        NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_z, 0));
+        NKR_TRY(msm_run(key->bases[k], key->scratch[k], z, out + kOutOffset[k], key->st[k]));
+        NKR_CUDA(cudaEventRecord(key->ev_done[k], key->st[k]));
+    }
+    // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
+    const NttTables &T = key->ntt;
+    const Fr *cst = T.consts.as<Fr>();
+    for (Fr *v : {az, bz, cz}) {
+        NKR_TRY(ntt_dif(T, v, true, nullptr, nullptr, nullptr, s0));
+        NKR_TRY(ntt_dit(T, v, false, T.t1.as<Fr>(), nullptr, nullptr, s0));
+    }
+    NKR_TRY(fr_quotient_pointwise(az, bz, cz, h, rows, cst + kConstZinv, s0));
+    NKR_TRY(ntt_dif(T, h, true, nullptr, T.t2.as<Fr>(), nullptr, s0));
+    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[2], s0));
+    NKR_TRY(msm_run(key->bases[kMsmH], key->scratch[kMsmH], h, out + kOutOffset[kMsmH], s0));
+    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[3], s0));
+    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2})
+        NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
+    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[4], s0));
+    return NKR_B200_OK;
+}
+
+int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_proving_key *pk,
+                nkr_b200_key **out)
+{
+    NKR_REQUIRE(ctx && c && pk && out, "null argument");
+    const int logn = log2_exact(c->rows);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "constraint count %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)c->rows);
+    NKR_REQUIRE(c->cols >= 1 && c->public_inputs + 1 <= c->cols,
+                "public input count exceeds the variable count");
+    for (int k = 0; k < 3; ++k)
+        NKR_REQUIRE(c->row_ptr[k] && (c->row_ptr[k][c->rows] == 0 || (c->col_idx[k] && c->values[k])),
+                    "matrix %d has null CSR arrays", k);
+    NKR_REQUIRE(pk->a_query && pk->b_g1_query && pk->b_g2_query && pk->l_query && pk->h_query &&
+                    pk->alpha_g1 && pk->beta_g1 && pk->delta_g1 && pk->beta_g2 && pk->delta_g2,
+                "proving key has null arrays");
+    NKR_CUDA(cudaSetDevice(ctx->device));
+    auto *key = new nkr_b200_key();
+    key->ctx = ctx;
+    key->rows = c->rows;
+    key->cols = c->cols;
+    key->public_inputs = c->public_inputs;
+    key->logn = logn;
+    auto fail = [&](int s) {
+        nkr_b200_key_free(key);
+        return s;
+    };
+    int s = NKR_B200_OK;
+#define NKR_PREP(expr)                                                                          \
+    do {                                                                                        \
+        s = (expr);                                                                             \
+        if (s != NKR_B200_OK) return fail(s);                                                   \
+    } while (0)
+    for (int k = 0; k < kNumMsm; ++k) {
+        if (cudaStreamCreateWithFlags(&key->st[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&key->ev_done[k], cudaEventDisableTiming) != cudaSuccess) {
+            set_error("stream/event creation failed");
+            return fail(NKR_B200_ECUDA);
+        }
+    }
+    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess) {
+        set_error("event creation failed");
+        return fail(NKR_B200_ECUDA);
+    }
+    for (auto &e : key->ev_t)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            set_error("event creation failed");
+            return fail(NKR_B200_ECUDA);
+        }
+    cudaStream_t st = key->st[kMsmH];
+    for (int k = 0; k < 3; ++k)
+        NKR_PREP(csr_upload(key->mat[k], c->rows, c->cols, c->row_ptr[k], c->col_idx[k],
+                            c->values[k], st));
+    NKR_PREP(ntt_tables_build(key->ntt, logn, st));
+    // proving key: normalise (hazard: CPU-setup keys are unnormalised Jacobian), fold windows
+    NKR_PREP(msm_bases_build(key->bases[kMsmA], 1, pk->a_query, false, c->cols, true, 0, false, st));
+    NKR_PREP(msm_bases_build(key->bases[kMsmB1], 1, pk->b_g1_query, false, c->cols, true, 0, false, st));
+    NKR_PREP(msm_bases_build(key->bases[kMsmL], 1, pk->l_query, false, c->cols, true, 0, false, st));
+    NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, 0, true, st));
+    NKR_PREP(msm_bases_build(key->bases[kMsmB2], 2, pk->b_g2_query, false, c->cols, true, 0, false, st));
+    for (int k = 0; k < kNumMsm; ++k)
+        NKR_PREP(msm_scratch_alloc(key->scratch[k], key->bases[k].group, key->bases[k].shape));
+    NKR_PREP(key->z.alloc(c->cols * 32, "witness"));
+    NKR_PREP(key->az.alloc(c->rows * 32, "az"));
+    NKR_PREP(key->bz.alloc(c->rows * 32, "bz"));
+    NKR_PREP(key->cz.alloc(c->rows * 32, "cz"));
+    NKR_PREP(key->h.alloc(c->rows * 32, "H"));
+    NKR_PREP(key->out.alloc(kOutBytes, "proof points"));
+    NKR_PREP(key->blind_io.alloc(64 + 384, "blinding io"));
+    // PK constants: libff Jacobian -> affine
+    {
+        DevBuf stage;
+        NKR_PREP(stage.alloc(3 * 96 + 2 * 192, "pk constant upload"));
+        uint8_t *sp = stage.as<uint8_t>();
+        const void *g1s[3] = {pk->alpha_g1, pk->beta_g1, pk->delta_g1};
+        const void *g2s[2] = {pk->beta_g2, pk->delta_g2};
+        for (int i = 0; i < 3; ++i)
+            if (cudaMemcpyAsync(sp + 96 * i, g1s[i], 96, cudaMemcpyHostToDevice, st) != cudaSuccess)
+                return fail(NKR_B200_ECUDA);
+        for (int i = 0; i < 2; ++i)
+            if (cudaMemcpyAsync(sp + 288 + 192 * i, g2s[i], 192, cudaMemcpyHostToDevice, st) !=
+                cudaSuccess)
+                return fail(NKR_B200_ECUDA);
+        NKR_PREP(key->pk_const.alloc(3 * sizeof(G1Affine) + 2 * sizeof(G2Affine), "pk constants"));
+        NKR_PREP(jacobian_to_affine(1, sp, key->pk_const.p, 3, st));
+        NKR_PREP(jacobian_to_affine(2, sp + 288, key->pk_const.as<uint8_t>() + 3 * sizeof(G1Affine), 2,
+                                    st));
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            set_error("prepare: %s", cudaGetErrorString(cudaGetLastError()));
+            return fail(NKR_B200_ECUDA);
+        }
+    }
+    if (cudaHostAlloc(&key->pinned_out, kOutBytes + 384, cudaHostAllocDefault) != cudaSuccess) {
+        set_error("pinned host allocation failed");
+        return fail(NKR_B200_ENOMEM);
+    }
+#undef NKR_PREP
+    *out = key;
+    return NKR_B200_OK;
+}
+
+int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_proof *res)
+{
+    NKR_REQUIRE(key && witness && res, "null argument");
+    NKR_REQUIRE(n == key->cols, "witness has %llu elements, the circuit has %llu columns",
+                (unsigned long long)n, (unsigned long long)key->cols);
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    cudaStream_t s0 = key->st[kMsmH];
+    // the previous prove's witness MSMs must be done before z is overwritten
+    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
+    cudaMemoryType mt;
+    check_witness_ptr(witness, &mt);
+    NKR_CUDA(cudaMemcpyAsync(key->z.p, witness, n * 32,
+                             mt == cudaMemoryTypeDevice ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyHostToDevice,
+                             s0));
+    NKR_TRY(prove_issue(key, true));
+    NKR_CUDA(cudaMemcpyAsync(key->pinned_out, key->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
+    NKR_CUDA(cudaStreamSynchronize(s0));
+    const uint8_t *o = static_cast<const uint8_t *>(key->pinned_out);
+    std::memcpy(res->ar, o + 0, 96);
+    std::memcpy(res->bs1, o + 96, 96);
+    std::memcpy(res->zk, o + 192, 96);
+    std::memcpy(res->qz, o + 288, 96);
+    std::memcpy(res->bs2, o + 384, 192);
+    float ms[4];
+    for (int i = 0; i < 4; ++i) NKR_CUDA(cudaEventElapsedTime(&ms[i], key->ev_t[i], key->ev_t[i + 1]));
+    key->times.spmv_ms = ms[0];
+    key->times.quotient_ms = ms[1];
+    key->times.quotient_msm_ms = ms[2];
+    NKR_CUDA(cudaEventElapsedTime(&key->times.total_ms, key->ev_t[0], key->ev_t[4]));
+    key->times.witness_msms_ms = key->times.total_ms - ms[0];
+    key->have_times = true;
+    return NKR_B200_OK;
+}
+
+int key_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r, const void *s,
+              nkr_b200_proof *res)
+{
+    NKR_REQUIRE(key && raw && r && s && res, "null argument");
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    cudaStream_t s0 = key->st[kMsmH];
+    uint8_t *host = static_cast<uint8_t *>(key->pinned_out) + kOutBytes; // 384 B staging
+    uint8_t *dev = key->blind_io.as<uint8_t>();
+    // raw points go to key->out (device) in libff layout; r, s to blind_io[0, 64)
+    uint8_t staging[kOutBytes];
+    std::memcpy(staging + 0, raw->ar, 96);
+    std::memcpy(staging + 96, raw->bs1, 96);
+    std::memcpy(staging + 192, raw->zk, 96);
+    std::memcpy(staging + 288, raw->qz, 96);
+    std::memcpy(staging + 384, raw->bs2, 192);
+    NKR_CUDA(cudaStreamSynchronize(s0));
+    NKR_CUDA(cudaMemcpy(key->out.p, staging, kOutBytes, cudaMemcpyHostToDevice));
+    NKR_CUDA(cudaMemcpy(dev, r, 32, cudaMemcpyHostToDevice));
+    NKR_CUDA(cudaMemcpy(dev + 32, s, 32, cudaMemcpyHostToDevice));
+    k_blind<<<1, 7 * 32, 0, s0>>>(key->pk_const.as<uint8_t>(), key->out.as<uint8_t>(),
+                              reinterpret_cast<const Fr *>(dev), dev + 64);
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaMemcpyAsync(host, dev + 64, 384, cudaMemcpyDeviceToHost, s0));
+    NKR_CUDA(cudaStreamSynchronize(s0));
+    std::memcpy(res->a, host, 96);
+    std::memcpy(res->b, host + 96, 192);
+    std::memcpy(res->c, host + 288, 96);
+    return NKR_B200_OK;
+}
+
+int key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
+{
+    NKR_REQUIRE(key, "null key");
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    cudaStream_t s0 = key->st[kMsmH];
+    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
+    const uint64_t rows = key->rows;
+    DevBuf tmp;
+    NKR_TRY(tmp.alloc(4 * rows * 32, "intermediate scratch"));
+    Fr *t = tmp.as<Fr>();
+    // the SpMV is a pure function of the resident witness: recompute az, bz, cz
+    const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
+    Fr *ys[3] = {t, t + rows, t + 2 * rows};
+    NKR_TRY(spmv_multi(mats, 3, key->z.as<Fr>(), ys, s0));
+    // H is held in bit-reversed order; return it in natural order
+    NKR_TRY(ntt_bitrev_permute(key->h.as<Fr>(), t + 3 * rows, rows, nullptr, nullptr, s0));
+    void *dst[4] = {az, bz, cz, h};
+    for (int i = 0; i < 4; ++i)
+        if (dst[i]) NKR_CUDA(cudaMemcpyAsync(dst[i], t + i * rows, rows * 32, cudaMemcpyDeviceToHost, s0));
+    NKR_CUDA(cudaStreamSynchronize(s0));
+    return NKR_B200_OK;
+}
+
+int key_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                    nkr_b200_raw_proof *out)
+{
+    NKR_REQUIRE(keys && witnesses && out && count >= 0, "null argument");
+    std::vector<std::vector<uint8_t>> staged(count);
+    // issue every proof without host synchronisation; proofs on different keys overlap
+    std::vector<void *> pinned(count, nullptr);
+    int status = NKR_B200_OK;
+    for (int i = 0; i < count && status == NKR_B200_OK; ++i) {
+        nkr_b200_key *key = keys[i];
+        if (!key) {
+            set_error("null key at %d", i);
+            status = NKR_B200_EINVAL;
+            break;
+        }
+        cudaSetDevice(key->ctx->device);
+        cudaStream_t s0 = key->st[kMsmH];
+        for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) cudaStreamWaitEvent(s0, key->ev_done[k], 0);
+        cudaMemoryType mt;
+        check_witness_ptr(witnesses[i], &mt);
+        if (cudaMemcpyAsync(key->z.p, witnesses[i], key->cols * 32,
+                            mt == cudaMemoryTypeDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            s0) != cudaSuccess) {
+            set_error("witness upload failed");
+            status = NKR_B200_ECUDA;
+            break;
+        }
+        status = prove_issue(key, false);
+        if (status != NKR_B200_OK) break;
+        if (cudaHostAlloc(&pinned[i], kOutBytes, cudaHostAllocDefault) != cudaSuccess) {
+            set_error("pinned allocation failed");
+            status = NKR_B200_ENOMEM;
+            break;
+        }
+        cudaMemcpyAsync(pinned[i], key->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0);
+    }
+    for (int i = 0; i < count; ++i) {
+        if (!pinned[i]) continue;
+        cudaStreamSynchronize(keys[i]->st[kMsmH]);
+        if (status == NKR_B200_OK) {
+            const uint8_t *o = static_cast<const uint8_t *>(pinned[i]);
+            std::memcpy(out[i].ar, o, 96);
+            std::memcpy(out[i].bs1, o + 96, 96);
+            std::memcpy(out[i].zk, o + 192, 96);
+            std::memcpy(out[i].qz, o + 288, 96);
+            std::memcpy(out[i].bs2, o + 384, 192);
+        }
+        cudaFreeHost(pinned[i]);
+    }
+    if (status == NKR_B200_OK) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            set_error("batch: %s", cudaGetErrorString(e));
+            status = NKR_B200_ECUDA;
+        }
+    }
+    return status;
+}
+
+} // namespace nkr
+
+void nkr_b200_key_free(nkr_b200_key *key)
+{
+    if (!key) return;
+    if (key->ctx) cudaSetDevice(key->ctx->device);
+    for (int k = 0; k < nkr::kNumMsm; ++k)
+        if (key->st[k]) cudaStreamSynchronize(key->st[k]);
+    for (int k = 0; k < nkr::kNumMsm; ++k) {
+        if (key->st[k]) cudaStreamDestroy(key->st[k]);
+        if (key->ev_done[k]) cudaEventDestroy(key->ev_done[k]);
+    }
+    if (key->ev_z) cudaEventDestroy(key->ev_z);
+    for (auto e : key->ev_t)
+        if (e) cudaEventDestroy(e);
+    if (key->pinned_out) cudaFreeHost(key->pinned_out);
+    if (key->pinned_in) cudaFreeHost(key->pinned_in);
+    delete key;
+}
+
+uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
+{
+    if (!key) return 0;
+    uint64_t b = key->ntt.device_bytes() + key->z.bytes + key->az.bytes + key->bz.bytes +
+                 key->cz.bytes + key->h.bytes + key->out.bytes + key->pk_const.bytes +
+                 key->blind_io.bytes;
+    for (int k = 0; k < 3; ++k)
+        b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].values.bytes;
+    for (int k = 0; k < nkr::kNumMsm; ++k)
+        b += key->bases[k].device_bytes() + key->scratch[k].device_bytes();
+    return b;
+}

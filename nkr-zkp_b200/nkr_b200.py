@@ -1,0 +1,394 @@
+"""ctypes binding of libnkr_b200.so (the C ABI in include/nkr_b200.h).
+
+Python mirror of the reference's Groth16 backend interface for the prove path
+(protocols/groth16/common/include/groth16/backend.hpp:11-28): `Backend.name()`,
+`prepare(circuit, proving_key)` and `prove(circuit, proving_key, witness)`
+returning a RawProof, plus the operator-level NTT / SpMV / MSM calls
+(operators/cuda/include/nkr/operators/cuda.hpp).  Buffers are numpy arrays in
+the reference's libff byte layouts (Fr = 4 x uint64 Montgomery; G1 Jacobian =
+12 x uint64; G2 Jacobian = 24 x uint64).
+
+There is no CPU fallback: importing this module fails loudly if the CUDA
+library has not been built, and every compute call raises if no sm_100 GPU is
+usable.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnkr_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python nkr-zkp_b200/build.py` "
+        "(there is no CPU fallback for the B200 backend)")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+OK, EINVAL, ECUDA, ENOMEM, ENODEV, ETIMEOUT, EBUSY = range(7)
+_VP = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+
+
+class Circuit(ctypes.Structure):
+    _fields_ = [("rows", _U64), ("cols", _U64), ("public_inputs", _U64),
+                ("row_ptr", _VP * 3), ("col_idx", _VP * 3), ("values", _VP * 3)]
+
+
+class ProvingKey(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("a_query", "b_g1_query", "b_g2_query", "l_query", "h_query",
+                                   "alpha_g1", "beta_g1", "delta_g1", "beta_g2", "delta_g2")]
+
+
+class RawProofC(ctypes.Structure):
+    _fields_ = [("ar", ctypes.c_uint8 * 96), ("bs1", ctypes.c_uint8 * 96),
+                ("zk", ctypes.c_uint8 * 96), ("qz", ctypes.c_uint8 * 96),
+                ("bs2", ctypes.c_uint8 * 192)]
+
+
+class ProofC(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_uint8 * 96), ("b", ctypes.c_uint8 * 192), ("c", ctypes.c_uint8 * 96)]
+
+
+class StageTimes(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in
+                ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms")]
+
+
+_SIGS = {
+    "nkr_b200_open": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP)]),
+    "nkr_b200_close": (None, [_VP]),
+    "nkr_b200_last_error": (ctypes.c_char_p, []),
+    "nkr_b200_backend_name": (ctypes.c_char_p, []),
+    "nkr_b200_prepare": (ctypes.c_int, [_VP, ctypes.POINTER(Circuit), ctypes.POINTER(ProvingKey),
+                                        ctypes.POINTER(_VP)]),
+    "nkr_b200_key_free": (None, [_VP]),
+    "nkr_b200_key_device_bytes": (_U64, [_VP]),
+    "nkr_b200_prove": (ctypes.c_int, [_VP, _VP, _U64, ctypes.POINTER(RawProofC)]),
+    "nkr_b200_blind": (ctypes.c_int, [_VP, ctypes.POINTER(RawProofC), _VP, _VP,
+                                      ctypes.POINTER(ProofC)]),
+    "nkr_b200_key_intermediates": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "nkr_b200_key_stage_times": (ctypes.c_int, [_VP, ctypes.POINTER(StageTimes)]),
+    "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
+                                            ctypes.POINTER(RawProofC)]),
+    "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
+    "nkr_b200_spmv": (ctypes.c_int, [_VP, _U64, _U64, _VP, _VP, _VP, _VP, _VP]),
+    "nkr_b200_msm_g1": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
+    "nkr_b200_msm_g2": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
+    "nkr_b200_msm_bases_create": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64, ctypes.POINTER(_VP)]),
+    "nkr_b200_msm_bases_run": (ctypes.c_int, [_VP, _VP, _U64, _VP, ctypes.POINTER(ctypes.c_float)]),
+    "nkr_b200_msm_bases_free": (None, [_VP]),
+    "nkr_b200_field_op": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _U64]),
+    "nkr_b200_group_op": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _U64]),
+    "nkr_b200_bench_mul": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double)]),
+    "nkr_b200_r1cs_generate": (ctypes.c_int, [ctypes.c_char_p, _U64, ctypes.c_int, _U64,
+                                              ctypes.POINTER(_VP)]),
+    "nkr_b200_r1cs_info": (ctypes.c_int, [_VP, ctypes.POINTER(_U64)]),
+    "nkr_b200_r1cs_view": (ctypes.c_int, [_VP, ctypes.POINTER(Circuit), ctypes.POINTER(_VP)]),
+    "nkr_b200_r1cs_free": (None, [_VP]),
+    "nkr_b200_poseidon_hash2": (ctypes.c_int, [_VP, _VP, _VP]),
+    "nkr_b200_poseidon_parameters": (ctypes.c_int, [_VP, _VP]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+class B200Error(RuntimeError):
+    def __init__(self, status, where):
+        msg = _lib.nkr_b200_last_error().decode(errors="replace")
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+def _check(status, where):
+    if status != OK:
+        raise B200Error(status, where)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_VP) if a is not None else None
+
+
+def _fr(a):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    assert a.size % 4 == 0
+    return a
+
+
+def lib():
+    return _lib
+
+
+def backend_name():
+    return _lib.nkr_b200_backend_name().decode()
+
+
+# ---------------------------------------------------------------------------
+# circuits (generated or given as numpy CSR arrays)
+# ---------------------------------------------------------------------------
+
+class R1CS:
+    """A circuit in the reference CSR layout plus its witness (numpy arrays)."""
+
+    def __init__(self, rows, cols, public_inputs, row_ptr, col_idx, values, witness):
+        self.rows, self.cols, self.public_inputs = int(rows), int(cols), int(public_inputs)
+        self.row_ptr = [np.ascontiguousarray(x, dtype=np.uint32) for x in row_ptr]
+        self.col_idx = [np.ascontiguousarray(x, dtype=np.uint32) for x in col_idx]
+        self.values = [_fr(x).reshape(-1, 4) for x in values]
+        self.witness = None if witness is None else _fr(witness).reshape(-1, 4)
+
+    def c_circuit(self):
+        c = Circuit()
+        c.rows, c.cols, c.public_inputs = self.rows, self.cols, self.public_inputs
+        for k in range(3):
+            c.row_ptr[k] = self.row_ptr[k].ctypes.data
+            c.col_idx[k] = self.col_idx[k].ctypes.data if self.col_idx[k].size else None
+            c.values[k] = self.values[k].ctypes.data if self.values[k].size else None
+        return c
+
+
+def generate(kind, param, density=0, seed=1):
+    """Seeded restatement of groth16-gen (kind: matmul, poseidon, sql-aggregate, fibonacci)."""
+    h = _VP()
+    _check(_lib.nkr_b200_r1cs_generate(kind.encode(), param, density, seed, ctypes.byref(h)),
+           f"generate {kind} {param}")
+    try:
+        sizes = (_U64 * 8)()
+        _check(_lib.nkr_b200_r1cs_info(h, sizes), "r1cs_info")
+        rows, cols, pub, ncons, nvars, na, nb, nc = list(sizes)
+        view = Circuit()
+        wit = _VP()
+        _check(_lib.nkr_b200_r1cs_view(h, ctypes.byref(view), ctypes.byref(wit)), "r1cs_view")
+
+        def arr(ptr, count, dtype, width=1):
+            if count == 0:
+                return np.zeros((0, width) if width > 1 else 0, dtype=dtype)
+            buf = (ctypes.c_uint8 * (count * width * np.dtype(dtype).itemsize)).from_address(ptr)
+            a = np.frombuffer(buf, dtype=dtype).copy()
+            return a.reshape(-1, width) if width > 1 else a
+
+        nnz = [na, nb, nc]
+        rp = [arr(view.row_ptr[k], rows + 1, np.uint32) for k in range(3)]
+        ci = [arr(view.col_idx[k], nnz[k], np.uint32) for k in range(3)]
+        vals = [arr(view.values[k], nnz[k], np.uint64, 4) for k in range(3)]
+        w = arr(wit.value, cols, np.uint64, 4)
+        r = R1CS(rows, cols, pub, rp, ci, vals, w)
+        r.constraints, r.variables = ncons, nvars
+        return r
+    finally:
+        _lib.nkr_b200_r1cs_free(h)
+
+
+def poseidon_hash2(left, right):
+    out = np.zeros(4, np.uint64)
+    _check(_lib.nkr_b200_poseidon_hash2(_ptr(_fr(left)), _ptr(_fr(right)), _ptr(out)), "poseidon")
+    return out
+
+
+def poseidon_parameters():
+    rc = np.zeros((195, 4), np.uint64)
+    mds = np.zeros((9, 4), np.uint64)
+    _check(_lib.nkr_b200_poseidon_parameters(_ptr(rc), _ptr(mds)), "poseidon_parameters")
+    return rc, mds
+
+
+# ---------------------------------------------------------------------------
+# device context, keys, operators
+# ---------------------------------------------------------------------------
+
+class Context:
+    """One GPU (nkr_b200_open)."""
+
+    def __init__(self, device=0):
+        h = _VP()
+        _check(_lib.nkr_b200_open(device, ctypes.byref(h)), "nkr_b200_open")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            _lib.nkr_b200_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # operator-level entry points -------------------------------------------
+    def ntt(self, op, data):
+        d = _fr(data).copy()
+        _check(_lib.nkr_b200_ntt(self.h, op, _ptr(d), d.size // 4), f"ntt op {op}")
+        return d.reshape(-1, 4)
+
+    def spmv(self, rows, cols, row_ptr, col_idx, values, z):
+        y = np.zeros((rows, 4), np.uint64)
+        rp = np.ascontiguousarray(row_ptr, np.uint32)
+        ci = np.ascontiguousarray(col_idx, np.uint32)
+        vv = _fr(values)
+        zz = _fr(z)
+        _check(_lib.nkr_b200_spmv(self.h, rows, cols, _ptr(rp), _ptr(ci) if ci.size else None,
+                                  _ptr(vv) if vv.size else None, _ptr(zz), _ptr(y)), "spmv")
+        return y
+
+    def msm(self, group, bases_jac, scalars):
+        b = np.ascontiguousarray(bases_jac, np.uint64)
+        s = _fr(scalars)
+        out = np.zeros(12 if group == 1 else 24, np.uint64)
+        f = _lib.nkr_b200_msm_g1 if group == 1 else _lib.nkr_b200_msm_g2
+        _check(f(self.h, _ptr(b), _ptr(s), s.size // 4, _ptr(out)), f"msm g{group}")
+        return out
+
+    def field_op(self, field, op, a, b=None):
+        w = 8 if field == 2 else 4
+        a = np.ascontiguousarray(a, np.uint64).reshape(-1, w)
+        bb = None if b is None else np.ascontiguousarray(b, np.uint64).reshape(-1, w)
+        out = np.zeros_like(a)
+        _check(_lib.nkr_b200_field_op(self.h, field, op, _ptr(a), _ptr(bb), _ptr(out), a.shape[0]),
+               f"field_op {field} {op}")
+        return out
+
+    def group_op(self, group, op, a, b=None):
+        w = 12 if group == 1 else 24
+        a = np.ascontiguousarray(a, np.uint64).reshape(-1, w)
+        bb = None if b is None else np.ascontiguousarray(b, np.uint64)
+        out = np.zeros_like(a)
+        _check(_lib.nkr_b200_group_op(self.h, group, op, _ptr(a), _ptr(bb), _ptr(out), a.shape[0]),
+               f"group_op {group} {op}")
+        return out
+
+    def bench_mul(self, field):
+        rate, ms = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.nkr_b200_bench_mul(self.h, field, ctypes.byref(rate), ctypes.byref(ms)),
+               "bench_mul")
+        return rate.value, ms.value
+
+
+class MsmBases:
+    """Resident MSM bases (per-window copies built once), then MSMs with new scalars."""
+
+    def __init__(self, ctx, group, bases_jac):
+        self.ctx, self.group = ctx, group
+        b = np.ascontiguousarray(bases_jac, np.uint64)
+        self.n = b.size // (12 if group == 1 else 24)
+        h = _VP()
+        _check(_lib.nkr_b200_msm_bases_create(ctx.h, group, _ptr(b), self.n, ctypes.byref(h)),
+               "msm_bases_create")
+        self.h = h
+
+    def run(self, scalars, scalars_ptr=None):
+        out = np.zeros(12 if self.group == 1 else 24, np.uint64)
+        ms = ctypes.c_float()
+        ptr = scalars_ptr if scalars_ptr is not None else _ptr(_fr(scalars))
+        _check(_lib.nkr_b200_msm_bases_run(self.h, ptr, self.n, _ptr(out), ctypes.byref(ms)),
+               "msm_bases_run")
+        return out, ms.value
+
+    def free(self):
+        if self.h:
+            _lib.nkr_b200_msm_bases_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def raw_to_arrays(raw):
+    g1 = [np.frombuffer(bytes(getattr(raw, f)), np.uint64).copy() for f in ("ar", "bs1", "zk", "qz")]
+    g2 = np.frombuffer(bytes(raw.bs2), np.uint64).copy()
+    return g1, g2
+
+
+class Backend:
+    """The B200 backend behind NKR-ZKP's Backend interface (prepare / prove).
+
+    Mirrors protocols/groth16/common/include/groth16/backend.hpp:11-28: prepare()
+    makes the circuit and proving key resident; prove() returns the raw proof
+    {ar, bs1, zk, qz, bs2} affine-normalised in libff layout.
+    """
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.key = None
+        self._keep = None
+
+    @staticmethod
+    def name():
+        return backend_name()
+
+    def prepare(self, r1cs, pk):
+        """pk: dict with a_query, b_g1_query, b_g2_query, l_query, h_query (uint64 arrays in
+        libff Jacobian layout) and alpha_g1, beta_g1, delta_g1, beta_g2, delta_g2."""
+        c = r1cs.c_circuit()
+        keep = {k: np.ascontiguousarray(v, np.uint64) for k, v in pk.items()}
+        p = ProvingKey()
+        for name, _ in ProvingKey._fields_:
+            setattr(p, name, keep[name].ctypes.data)
+        h = _VP()
+        _check(_lib.nkr_b200_prepare(self.ctx.h, ctypes.byref(c), ctypes.byref(p), ctypes.byref(h)),
+               "nkr_b200_prepare")
+        self.free()
+        self.key = h
+        self._keep = keep
+        self.cols = r1cs.cols
+        self.rows = r1cs.rows
+
+    def prove(self, witness, witness_ptr=None):
+        raw = RawProofC()
+        if witness_ptr is None:
+            w = _fr(witness)
+            _check(_lib.nkr_b200_prove(self.key, _ptr(w), w.size // 4, ctypes.byref(raw)),
+                   "nkr_b200_prove")
+        else:
+            _check(_lib.nkr_b200_prove(self.key, witness_ptr, self.cols, ctypes.byref(raw)),
+                   "nkr_b200_prove")
+        return raw
+
+    def blind(self, raw, r, s):
+        proof = ProofC()
+        _check(_lib.nkr_b200_blind(self.key, ctypes.byref(raw), _ptr(_fr(r)), _ptr(_fr(s)),
+                                   ctypes.byref(proof)), "nkr_b200_blind")
+        return proof
+
+    def intermediates(self):
+        az, bz, cz, h = (np.zeros((self.rows, 4), np.uint64) for _ in range(4))
+        _check(_lib.nkr_b200_key_intermediates(self.key, _ptr(az), _ptr(bz), _ptr(cz), _ptr(h)),
+               "intermediates")
+        return az, bz, cz, h
+
+    def stage_times(self):
+        t = StageTimes()
+        _check(_lib.nkr_b200_key_stage_times(self.key, ctypes.byref(t)), "stage_times")
+        return {n: getattr(t, n) for n, _ in StageTimes._fields_}
+
+    def device_bytes(self):
+        return int(_lib.nkr_b200_key_device_bytes(self.key))
+
+    def free(self):
+        if self.key:
+            _lib.nkr_b200_key_free(self.key)
+            self.key = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def prove_batch(backends, witnesses):
+    n = len(backends)
+    keys = (_VP * n)(*[b.key for b in backends])
+    ws = [_fr(w) for w in witnesses]
+    wp = (_VP * n)(*[w.ctypes.data for w in ws])
+    out = (RawProofC * n)()
+    _check(_lib.nkr_b200_prove_batch(keys, wp, n, out), "prove_batch")
+    return list(out)

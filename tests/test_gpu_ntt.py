@@ -1,0 +1,61 @@
+"""NTT / domain operations on the B200 against libfqfft's semantics (the oracle
+restates basic_radix2_domain; golden digests come from the reference's own
+libfqfft).  Bit-exact: outputs are unique field vectors."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("logn", [1, 2, 3, 5, 8, 10, 11, 12, 16])
+def test_domain_ops_match_oracle(ctx, orc, logn, rng):
+    n = 1 << logn
+    x = O.random_fr(n, rng)
+    x[0] = 0
+    for op in range(5):
+        assert np.array_equal(ctx.ntt(op, x), orc.domain_op(op, x)), f"op {op} n 2^{logn}"
+
+
+def test_domain_ops_golden(ctx):
+    g = json.load(open(os.path.join(GOLDEN, "domain_ops.json")))
+    x = O.random_fr(g["n"], np.random.default_rng(g["seed"]))
+    for op, digest in g["ops"].items():
+        assert O.sha256_arr(ctx.ntt(int(op), x)) == digest, f"op {op}"
+
+
+@pytest.mark.parametrize("logn", [20, 22])
+def test_large_round_trips_and_spot_values(ctx, logn, rng):
+    """Size-independent properties at the benchmark sizes: inverse pairs are
+    identities, linearity holds, and sampled outputs equal the definition
+    sum_i a_i w^(ij)."""
+    n = 1 << logn
+    x = O.random_fr(n, rng)
+    f = ctx.ntt(0, x)
+    assert np.array_equal(ctx.ntt(1, f), x)
+    c = ctx.ntt(2, x)
+    assert np.array_equal(ctx.ntt(3, c), x)
+    # linearity: FFT(x + y) = FFT(x) + FFT(y) on a sample of coordinates
+    y = O.random_fr(n, rng)
+    fy = ctx.ntt(0, y)
+    s = np.stack([O.fr_mont((O.fr_int(x[i]) + O.fr_int(y[i])) % O.R) for i in range(n)]) if logn <= 20 else None
+    if s is not None:
+        fs = ctx.ntt(0, s)
+        for j in rng.integers(0, n, 8):
+            assert O.fr_int(fs[j]) == (O.fr_int(f[j]) + O.fr_int(fy[j])) % O.R
+    # definition at two sampled points (w = 5^((r-1)/2^28) squared down)
+    w = pow(pow(5, (O.R - 1) >> 28, O.R), 1 << (28 - logn), O.R)
+    xi = [O.fr_int(v) for v in x] if logn <= 20 else None
+    if xi is not None:
+        for j in (1, int(rng.integers(2, n))):
+            wj = pow(w, j, O.R)
+            acc, p = 0, 1
+            for a in xi:
+                acc = (acc + a * p) % O.R
+                p = p * wj % O.R
+            assert O.fr_int(f[j]) == acc

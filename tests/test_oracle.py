@@ -1,0 +1,147 @@
+"""The C restatement (oracle/bn254_oracle.c) pinned against the reference: its
+known-answer vectors, the golden fixtures made by the reference's own code
+(tests/golden/make_golden.py), and, where oracle/_ref is built, direct
+comparisons with the reference CPU path on fresh seeded inputs."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN
+
+
+def test_fr_constants(orc):
+    # one, multiplicative generator 5, 2^28-th root of unity (alt_bn128_init.cpp:56-61)
+    assert O.fr_int(orc.fr_constant(0)) == 1
+    assert O.fr_int(orc.fr_constant(1)) == 5
+    w = O.fr_int(orc.fr_constant(2))
+    assert pow(w, 2**28, O.R) == 1 and pow(w, 2**27, O.R) != 1
+    assert w == pow(5, (O.R - 1) >> 28, O.R)
+
+
+def test_field_ops_match_bigint(orc, rng):
+    for which, mod in ((0, O.R), (1, O.P)):
+        conv = O.fr_mont if which == 0 else O.fq_mont
+        back = O.fr_int if which == 0 else O.fq_int
+        vals = [0, 1, mod - 1, 2**255 % mod] + [int(rng.integers(0, 2**62)) ** 4 % mod for _ in range(20)]
+        for a in vals:
+            for b in vals[:6]:
+                assert back(orc.fe("mul", which, conv(a), conv(b))) == a * b % mod
+                assert back(orc.fe("add", which, conv(a), conv(b))) == (a + b) % mod
+                assert back(orc.fe("sub", which, conv(a), conv(b))) == (a - b) % mod
+            if a:
+                assert back(orc.fe("inv", which, conv(a))) == pow(a, -1, mod)
+
+
+def test_poseidon_known_answer(orc):
+    g = json.load(open(os.path.join(GOLDEN, "poseidon_constants.json")))
+    rc = np.stack([O.fr_mont(int(x, 16)) for x in g["round_constants"]])
+    mds = np.stack([O.fr_mont(int(x, 16)) for x in g["mds"]])
+    d = orc.poseidon_hash2(rc, mds, O.fr_mont(1), O.fr_mont(2))
+    # protocols/groth16/tests/poseidon_test.cpp:21-24
+    assert O.fr_int(d) == 7853200120776062878684798364095072458815029376092732009249414926327459813530
+    assert str(O.fr_int(d)) == g["hash2_1_2"]
+
+
+def test_domain_ops_golden(orc):
+    g = json.load(open(os.path.join(GOLDEN, "domain_ops.json")))
+    x = O.random_fr(g["n"], np.random.default_rng(g["seed"]))
+    assert O.sha256_arr(x) == g["input_sha256"]
+    for op, digest in g["ops"].items():
+        assert O.sha256_arr(orc.domain_op(int(op), x)) == digest, f"op {op}"
+
+
+def _msm_inputs(orc, group, n, seed):
+    # mirrors make_golden.msm_inputs; bases from the oracle's own scalar multiples
+    r = np.random.default_rng(seed)
+    ks = O.random_fr(n, r)
+    sc = O.random_fr(n, r)
+    sc[0] = 0
+    sc[1] = O.fr_mont(1)
+    sc[2] = O.fr_mont(O.R - 1)
+    sc[3] = sc[4]
+    ks[3] = ks[4]
+    sc[5] = O.fr_mont(2**16 - 1)
+    gen = orc.g1_generator() if group == 1 else orc.g2_generator()
+    aff = np.stack([orc.mul_affine(group, gen, k) for k in ks])
+    aff[6] = 0
+    aff[6, 4 * group:4 * group + 4] = O.fq_mont(1)
+    return aff, sc
+
+
+@pytest.mark.parametrize("group", [1, 2])
+def test_msm_golden(orc, group):
+    g = json.load(open(os.path.join(GOLDEN, "msm.json")))[f"g{group}"]
+    aff, sc = _msm_inputs(orc, group, g["n"], g["seed"])
+    assert O.sha256_arr(O.affine_to_jac(group, aff)) == g["bases_sha256"]
+    res = orc.msm(group, aff, sc)
+    assert res.tobytes().hex() == g["result_affine"]
+
+
+def _pk_affine(orc, pk):
+    return O.pk_affine(pk, orc)
+
+
+def test_prove_golden_matmul4(orc):
+    import nkr_b200 as nk
+    g = json.load(open(os.path.join(GOLDEN, "matmul4.json")))
+    r1 = nk.generate(g["kind"], g["param"], g["density"], seed=g["seed"])
+    assert O.sha256_arr(r1.witness) == g["witness_sha256"]
+    pk = O.read_proving_key(os.path.join(GOLDEN, "matmul4.pk.bin"))
+    g1, g2 = orc.prove(r1, _pk_affine(orc, pk), r1.witness)
+    assert [g1[i].tobytes().hex() for i in range(4)] == g["raw_g1_affine"]
+    assert g2.tobytes().hex() == g["raw_g2_affine"]
+
+
+# ---- direct comparisons with the reference CPU path (oracle/_ref) -----------
+
+@pytest.mark.parametrize("n", [2, 4, 256, 2048])
+def test_domain_ops_vs_ref(orc, ref, n, rng):
+    x = O.random_fr(n, rng)
+    for op in range(5):
+        assert np.array_equal(orc.domain_op(op, x), ref.domain_op(op, x)), f"op {op} n {n}"
+
+
+@pytest.mark.parametrize("group,n", [(1, 1), (1, 3), (1, 500), (2, 40)])
+def test_msm_vs_ref(orc, ref, group, n, rng):
+    ks = O.random_fr(n, rng)
+    sc = O.random_fr(n, rng)
+    if n > 3:
+        sc[: n // 4] = 0  # sparse witness
+    jac = np.stack([ref.mul_gen(group, k) for k in ks])
+    aff = orc.to_affine(group, jac)
+    assert np.array_equal(orc.msm(group, aff, sc), ref.multiexp(group, jac, sc)[:8 * group])
+
+
+def test_prove_and_setup_scalars_vs_ref(orc, ref, tmp_path):
+    import nkr_b200 as nk
+    r1 = nk.generate("poseidon", 2, 1, seed=9)
+    pk_path, vk_path = tmp_path / "p.pk.bin", tmp_path / "p.vk.bin"
+    ref.cpu_setup(r1, pk_path, vk_path)
+    pk = O.read_proving_key(pk_path)
+    g1, g2 = orc.prove(r1, _pk_affine(orc, pk), r1.witness)
+    rg1, rg2 = ref.cpu_prove(r1, pk_path, r1.witness)
+    assert np.array_equal(g1, rg1) and np.array_equal(g2, rg2)
+
+
+def test_blind_then_reference_verify(orc, ref, tmp_path):
+    """Oracle blinding with seeded r, s gives a proof the reference verifier accepts."""
+    import nkr_b200 as nk
+    g = json.load(open(os.path.join(GOLDEN, "matmul4.json")))
+    r1 = nk.generate(g["kind"], g["param"], g["density"], seed=g["seed"])
+    pk = O.read_proving_key(os.path.join(GOLDEN, "matmul4.pk.bin"))
+    pka = _pk_affine(orc, pk)
+    g1, g2 = orc.prove(r1, pka, r1.witness)
+    rng = np.random.default_rng(77)
+    r, s = O.random_fr(2, rng)
+    a, b, c = orc.blind(pka, g1, g2, r, s)
+    path = tmp_path / "proof.bin"
+    O.write_proof(path, O.affine_to_jac(1, a), O.affine_to_jac(2, b), O.affine_to_jac(1, c))
+    pub = r1.witness[1:1 + r1.public_inputs]
+    assert ref.verify(os.path.join(GOLDEN, "matmul4.vk.bin"), pub, path)
+    # a tampered proof must fail
+    c2 = orc.add_affine(1, c, orc.g1_generator())
+    O.write_proof(path, O.affine_to_jac(1, a), O.affine_to_jac(2, b), O.affine_to_jac(1, c2))
+    assert not ref.verify(os.path.join(GOLDEN, "matmul4.vk.bin"), pub, path)
