@@ -160,6 +160,20 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
                            float *device_ms);
 void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b);
 
+/* Statistics of the last nkr_b200_msm_bases_run: device time of the whole MSM
+ * and of the bucket-accumulation kernel (CUDA events on its stream), the number
+ * of (point, nonzero digit) entries it accumulated, accumulation tasks, window
+ * shape and bucket count. */
+typedef struct {
+    float total_ms, acc_ms;
+    uint64_t entries, tasks;
+    uint32_t window_bits, windows, buckets;
+} nkr_b200_msm_stats;
+int nkr_b200_msm_bases_stats(const nkr_b200_msm_bases *b, nkr_b200_msm_stats *out);
+
+/* Kernels this library has launched in this process (for launch accounting). */
+uint64_t nkr_b200_launch_count(void);
+
 /* ---- field / group primitives (tests and microbenchmarks) ------------------ */
 
 /* Elementwise field op over n pairs (host buffers): field 0 Fr, 1 Fq, 2 Fq2;
@@ -173,6 +187,26 @@ int nkr_b200_group_op(nkr_b200_ctx *ctx, int group, int op, const void *a, const
 /* Throughput microbenchmark of the Montgomery product: field 0 Fr, 1 Fq.
  * Returns products per second and 32-bit IMAD-class instructions per product. */
 int nkr_b200_bench_mul(nkr_b200_ctx *ctx, int field, double *muls_per_s, double *ms);
+
+/* ---- setup ------------------------------------------------------------------ */
+
+/* Caller-allocated outputs of nkr_b200_setup, libff Jacobian layout (Z = 1). */
+typedef struct {
+    void *a_query, *b_g1_query, *l_query; /* G1[cols] */
+    void *b_g2_query;                     /* G2[cols] */
+    void *h_query;                        /* G1[rows] */
+    void *ic;                             /* G1[public_inputs + 1] (verification key) */
+    void *alpha_g1, *beta_g1, *delta_g1;  /* G1 */
+    void *beta_g2, *delta_g2, *gamma_g2;  /* G2 */
+} nkr_b200_setup_out;
+
+/* Groth16 setup with given toxic waste Fr[5] = {t, alpha, beta, gamma, delta}
+ * (Montgomery): query scalars on the host, fixed-base multiples on the GPU.
+ * Replaces Backend::setup (backends/cpu/src/backend.cpp:41-154; CUDA
+ * groth16_backend.cu:105-212) except the VK pairing e(alpha, beta), which the
+ * verifier side forms from alpha_g1 and beta_g2. */
+int nkr_b200_setup(nkr_b200_ctx *ctx, const nkr_b200_circuit *circuit, const void *toxic,
+                   const nkr_b200_setup_out *out);
 
 /* ---- seeded circuit + witness generators --------------------------------- */
 

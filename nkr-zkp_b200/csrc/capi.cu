@@ -16,6 +16,8 @@
 
 namespace nkr {
 
+std::atomic<unsigned long long> g_kernel_launches{0};
+
 namespace {
 thread_local char g_err[1024] = "";
 std::mutex g_table_mu;
@@ -109,6 +111,7 @@ struct nkr_b200_msm_bases {
     nkr::MsmBases bases;
     nkr::MsmScratch scratch;
     nkr::DevBuf scalars;
+    nkr_b200_msm_stats last{};
 };
 
 using namespace nkr;
@@ -116,6 +119,7 @@ using namespace nkr;
 extern "C" {
 
 const char *nkr_b200_last_error(void) { return get_error(); }
+uint64_t nkr_b200_launch_count(void) { return g_kernel_launches.load(); }
 const char *nkr_b200_backend_name(void) { return "b200"; }
 
 int nkr_b200_open(int device, nkr_b200_ctx **out)
@@ -306,6 +310,9 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     h->ctx = ctx;
     NKR_TRY(msm_bases_build(h->bases, group, bases, false, n, true, 0, false, ctx->stream));
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
+    NKR_CUDA(cudaEventCreate(&h->scratch.ev_acc[0]));
+    NKR_CUDA(cudaEventCreate(&h->scratch.ev_acc[1]));
+    h->scratch.timing = true;
     NKR_TRY(h->scalars.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
     *out = h.release();
     return NKR_B200_OK;
@@ -341,10 +348,32 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
     NKR_CUDA(cudaMemcpyAsync(out, b->scratch.result.p, b->bases.group == 1 ? 96 : 192,
                              cudaMemcpyDeviceToHost, st));
     NKR_CUDA(cudaStreamSynchronize(st));
-    if (device_ms) cudaEventElapsedTime(device_ms, e0, e1);
+    float total = 0.f;
+    cudaEventElapsedTime(&total, e0, e1);
+    if (device_ms) *device_ms = total;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (s == NKR_B200_OK) {
+        b->last.total_ms = total;
+        NKR_CUDA(cudaEventElapsedTime(&b->last.acc_ms, b->scratch.ev_acc[0], b->scratch.ev_acc[1]));
+        uint32_t entries = 0, tasks = 0;
+        const uint32_t nb = b->bases.shape.nb;
+        NKR_CUDA(cudaMemcpy(&entries, b->scratch.offsets.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
+        NKR_CUDA(cudaMemcpy(&tasks, b->scratch.task_off.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
+        b->last.entries = entries;
+        b->last.tasks = tasks;
+        b->last.window_bits = uint32_t(b->bases.shape.c);
+        b->last.windows = uint32_t(b->bases.shape.W);
+        b->last.buckets = nb;
+    }
     return s;
+}
+
+int nkr_b200_msm_bases_stats(const nkr_b200_msm_bases *b, nkr_b200_msm_stats *out)
+{
+    NKR_REQUIRE(b && out, "null argument");
+    *out = b->last;
+    return NKR_B200_OK;
 }
 
 void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
@@ -352,6 +381,8 @@ void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
     if (!b) return;
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
+    for (auto &e : b->scratch.ev_acc)
+        if (e) cudaEventDestroy(e);
     delete b;
 }
 

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -34,7 +35,14 @@ const char *get_error();
         if (nkr_s_ != NKR_B200_OK) return nkr_s_;                                               \
     } while (0)
 
-#define NKR_CHECK_LAUNCH() NKR_CUDA(cudaGetLastError())
+// Every kernel launch is followed by exactly one NKR_CHECK_LAUNCH(): it counts
+// the launch (nkr_b200_launch_count) and surfaces launch errors.
+extern std::atomic<unsigned long long> g_kernel_launches;
+#define NKR_CHECK_LAUNCH()                                                                      \
+    do {                                                                                        \
+        ::nkr::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);                       \
+        NKR_CUDA(cudaGetLastError());                                                           \
+    } while (0)
 
 #define NKR_REQUIRE(cond, ...)                                                                  \
     do {                                                                                        \

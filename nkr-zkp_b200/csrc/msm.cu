@@ -358,6 +358,7 @@ int build_windows_t(MsmBases &b, cudaStream_t st)
     for (int k = 1; k < sh.W; ++k) {
         k_dbl_c<F><<<blocks_for(sh.n, 128), 128, 0, st>>>(pts + uint64_t(k - 1) * sh.n,
                                                           tmp.as<Xyzz<F>>(), sh.n, sh.c);
+        NKR_CHECK_LAUNCH();
         k_xyzz_to_affine<F><<<blocks_for(chunks, 64), 64, 0, st>>>(tmp.as<Xyzz<F>>(),
                                                                    pts + uint64_t(k) * sh.n, sh.n);
         NKR_CHECK_LAUNCH();
@@ -394,11 +395,13 @@ int msm_run_t(const MsmBases &bs, MsmScratch &s, const void *scalars_dev, void *
     }
     const uint64_t tmax = sh.tasks_max();
     const unsigned tb = blocks_for(tmax, 128);
+    if (s.timing) NKR_CUDA(cudaEventRecord(s.ev_acc[0], st));
     k_acc_l1<F><<<tb, 128, 0, st>>>(s.task_off.as<uint32_t>(), s.offsets.as<uint32_t>(),
                                     s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, sh.k1,
                                     s.task_bucket.as<uint32_t>(), s.partials.as<Xyzz<F>>(),
                                     s.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
+    if (s.timing) NKR_CUDA(cudaEventRecord(s.ev_acc[1], st));
     // fix-up levels until one task's fan-in covers the largest possible bucket
     for (uint64_t stride = 1; stride < tmax; stride *= uint64_t(sh.k2)) {
         k_acc_up<F><<<tb, 128, 0, st>>>(s.task_off.as<uint32_t>(), sh.nb,

@@ -50,6 +50,8 @@ MsmShape msm_shape(uint64_t n, bool folded, int group, int c_override = 0);
 struct MsmScratch {
     DevBuf canon, counts, offsets, cursor, task_off, entries, task_bucket, partials, buckets;
     DevBuf red_a, red_r, red_a2, red_r2, scan_tmp, result;
+    bool timing = false;            // record events around the level-1 accumulation kernel
+    cudaEvent_t ev_acc[2] = {nullptr, nullptr};
     size_t device_bytes() const
     {
         return canon.bytes + counts.bytes + offsets.bytes + cursor.bytes + task_off.bytes +

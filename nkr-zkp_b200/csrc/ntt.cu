@@ -232,17 +232,25 @@ int ntt_tables_build(NttTables &t, int logn, cudaStream_t st)
     NKR_TRY(tmp.alloc(bytes, "ntt table scratch"));
     Fr *c = t.consts.as<Fr>();
     k_ntt_constants<<<1, 32, 0, st>>>(logn, c);
+    NKR_CHECK_LAUNCH();
     const unsigned pb = blocks_for((t.n + kPowRun - 1) / kPowRun, 128);
     const unsigned nb = blocks_for(t.n, 256);
     // forward stage twiddles from powers of w (tmp holds w^i, i < N/2)
     k_powers<<<pb, 128, 0, st>>>(c + kConstOmega, tmp.as<Fr>(), t.n / 2);
+    NKR_CHECK_LAUNCH();
     k_stage_twiddles<<<nb, 256, 0, st>>>(tmp.as<Fr>(), t.tw_fwd.as<Fr>(), logn);
+    NKR_CHECK_LAUNCH();
     k_powers<<<pb, 128, 0, st>>>(c + kConstOmegaInv, tmp.as<Fr>(), t.n / 2);
+    NKR_CHECK_LAUNCH();
     k_stage_twiddles<<<nb, 256, 0, st>>>(tmp.as<Fr>(), t.tw_inv.as<Fr>(), logn);
+    NKR_CHECK_LAUNCH();
     // g^i natural, then the bit-reversed scale tables
     k_powers<<<pb, 128, 0, st>>>(c + kConstG, t.gpow.as<Fr>(), t.n);
+    NKR_CHECK_LAUNCH();
     k_bitrev_scaled<<<nb, 256, 0, st>>>(t.gpow.as<Fr>(), c + kConstNinv, t.t1.as<Fr>(), logn);
+    NKR_CHECK_LAUNCH();
     k_powers<<<pb, 128, 0, st>>>(c + kConstGinv, tmp.as<Fr>(), t.n);
+    NKR_CHECK_LAUNCH();
     k_bitrev_scaled<<<nb, 256, 0, st>>>(tmp.as<Fr>(), c + kConstNinv, t.t2.as<Fr>(), logn);
     NKR_CHECK_LAUNCH();
     NKR_CUDA(cudaStreamSynchronize(st));

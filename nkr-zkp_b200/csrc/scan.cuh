@@ -101,7 +101,9 @@ int scan_exclusive(Load load, uint64_t n, uint32_t *out, uint32_t *scratch, cuda
     NKR_REQUIRE(nb <= uint32_t(kScanTile), "scan of %llu elements exceeds the two-level limit",
                 (unsigned long long)n);
     k_scan_totals<<<nb, kScanThreads, 0, st>>>(load, n, scratch);
+    NKR_CHECK_LAUNCH();
     k_scan_block_totals<<<1, kScanThreads, 0, st>>>(scratch, nb);
+    NKR_CHECK_LAUNCH();
     k_scan_apply<<<nb, kScanThreads, 0, st>>>(load, n, scratch, out);
     NKR_CHECK_LAUNCH();
     return NKR_B200_OK;

@@ -57,7 +57,15 @@ class StageTimes(ctypes.Structure):
                 ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms")]
 
 
+class MsmStats(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_float), ("acc_ms", ctypes.c_float), ("entries", _U64),
+                ("tasks", _U64), ("window_bits", ctypes.c_uint32), ("windows", ctypes.c_uint32),
+                ("buckets", ctypes.c_uint32)]
+
+
 _SIGS = {
+    "nkr_b200_launch_count": (_U64, []),
+    "nkr_b200_msm_bases_stats": (ctypes.c_int, [_VP, ctypes.POINTER(MsmStats)]),
     "nkr_b200_open": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP)]),
     "nkr_b200_close": (None, [_VP]),
     "nkr_b200_last_error": (ctypes.c_char_p, []),
@@ -126,6 +134,11 @@ def lib():
 
 def backend_name():
     return _lib.nkr_b200_backend_name().decode()
+
+
+def launch_count():
+    """Kernels launched by the library so far in this process."""
+    return int(_lib.nkr_b200_launch_count())
 
 
 # ---------------------------------------------------------------------------
@@ -289,6 +302,11 @@ class MsmBases:
                "msm_bases_run")
         return out, ms.value
 
+    def stats(self):
+        s = MsmStats()
+        _check(_lib.nkr_b200_msm_bases_stats(self.h, ctypes.byref(s)), "msm_bases_stats")
+        return {n: getattr(s, n) for n, _ in MsmStats._fields_}
+
     def free(self):
         if self.h:
             _lib.nkr_b200_msm_bases_free(self.h)
@@ -382,6 +400,43 @@ class Backend:
             self.free()
         except Exception:
             pass
+
+
+class SetupOut(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("a_query", "b_g1_query", "l_query", "b_g2_query", "h_query", "ic",
+                                   "alpha_g1", "beta_g1", "delta_g1", "beta_g2", "delta_g2",
+                                   "gamma_g2")]
+
+
+_lib.nkr_b200_setup.restype = ctypes.c_int
+_lib.nkr_b200_setup.argtypes = [_VP, ctypes.POINTER(Circuit), _VP, ctypes.POINTER(SetupOut)]
+
+
+def setup(ctx, r1cs, toxic):
+    """GPU setup with toxic waste Fr[5] = (t, alpha, beta, gamma, delta).
+
+    Returns (pk, vk_parts): pk in the proving-key dict layout Backend.prepare takes
+    (libff Jacobian arrays); vk_parts holds ic, gamma_g2, delta_g2, alpha_g1, beta_g2."""
+    cols, rows = r1cs.cols, r1cs.rows
+    arrs = {
+        "a_query": np.zeros((cols, 12), np.uint64), "b_g1_query": np.zeros((cols, 12), np.uint64),
+        "l_query": np.zeros((cols, 12), np.uint64), "b_g2_query": np.zeros((cols, 24), np.uint64),
+        "h_query": np.zeros((rows, 12), np.uint64),
+        "ic": np.zeros((r1cs.public_inputs + 1, 12), np.uint64),
+        "alpha_g1": np.zeros(12, np.uint64), "beta_g1": np.zeros(12, np.uint64),
+        "delta_g1": np.zeros(12, np.uint64), "beta_g2": np.zeros(24, np.uint64),
+        "delta_g2": np.zeros(24, np.uint64), "gamma_g2": np.zeros(24, np.uint64),
+    }
+    out = SetupOut()
+    for name, _ in SetupOut._fields_:
+        setattr(out, name, arrs[name].ctypes.data)
+    c = r1cs.c_circuit()
+    tox = _fr(np.stack([np.asarray(t, np.uint64) for t in toxic]))
+    _check(_lib.nkr_b200_setup(ctx.h, ctypes.byref(c), _ptr(tox), ctypes.byref(out)), "nkr_b200_setup")
+    pk = {k: arrs[k] for k in ("a_query", "b_g1_query", "b_g2_query", "l_query", "h_query",
+                               "alpha_g1", "beta_g1", "delta_g1", "beta_g2", "delta_g2")}
+    vk = {k: arrs[k] for k in ("ic", "gamma_g2", "delta_g2", "alpha_g1", "beta_g2")}
+    return pk, vk
 
 
 def prove_batch(backends, witnesses):

@@ -367,6 +367,13 @@ class Ref:
         c = _arr(cats)
         return self._build(self.lib.ref_sql_circuit, _U64(c.size // 4), _p(c), _p(_arr(amts)))
 
+    def write_vk(self, vk_parts, path):
+        """Verification key artifact for keys made elsewhere; e(alpha, beta) by libff."""
+        ic = _arr(vk_parts["ic"])
+        self._ok(self.lib.ref_write_vk(_p(_arr(vk_parts["alpha_g1"])), _p(_arr(vk_parts["beta_g2"])),
+                                       _p(_arr(vk_parts["gamma_g2"])), _p(_arr(vk_parts["delta_g2"])),
+                                       _p(ic), _U64(ic.size // 12), str(path).encode()), "write_vk")
+
     def poseidon_circuit(self, left, right):
         rows, cols = _U64(), _U64()
         nnz = (_U64 * 3)()

@@ -518,3 +518,29 @@ int ref_sql_circuit(uint64_t n, const void *cat_raw, const void *amt_raw, uint64
 }
 
 } // extern "C"
+
+extern "C" {
+
+// Writes a reference verification key artifact (io.cpp:79-84) for keys made
+// elsewhere: the reference computes e(alpha_g1, beta_g2) with its own pairing.
+// Inputs in libff layout; ic holds n_ic G1 points.
+int ref_write_vk(const void *alpha_g1, const void *beta_g2, const void *gamma_g2,
+                 const void *delta_g2, const void *ic, uint64_t n_ic, const char *path)
+{
+    REF_TRY({
+        G1 a;
+        G2 b, g, d;
+        std::memcpy((void *)&a, alpha_g1, 96);
+        std::memcpy((void *)&b, beta_g2, 192);
+        std::memcpy((void *)&g, gamma_g2, 192);
+        std::memcpy((void *)&d, delta_g2, 192);
+        VerificationKey vk;
+        vk.alpha_g1_beta_g2 = Curve::reduced_pairing(a, b);
+        vk.gamma_g2 = g;
+        vk.delta_g2 = d;
+        vk.ic = from_raw<G1>(ic, n_ic);
+        write_verification_key(path, vk);
+    })
+}
+
+} // extern "C"
