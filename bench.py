@@ -329,7 +329,7 @@ def run_b200(args):
         achieved = muls / (acc_ms * 1e-3)
         # algorithmic HBM bytes of the launch: one 64 B affine base + 4 B entry per entry,
         # plus the task bucket ids and bucket / partial writes (128 B each)
-        algo_bytes = st["entries"] * (64 + 4) + st["tasks"] * (4 + 128)
+        algo_bytes = st["entries"] * (64 + 4) + st["tasks"] * 2 * 128
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         roof = {"bound": "int", "kernel": "k_acc_l1<Fq> (G1 bucket accumulation)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),

@@ -184,8 +184,9 @@ int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const
  * op 0 add, 1 double (b ignored), 2 scalar multiple by Fr b (Montgomery). */
 int nkr_b200_group_op(nkr_b200_ctx *ctx, int group, int op, const void *a, const void *b,
                       void *out, uint64_t n);
-/* Throughput microbenchmark of the Montgomery product: field 0 Fr, 1 Fq.
- * Returns products per second and 32-bit IMAD-class instructions per product. */
+/* Throughput microbenchmark of the Montgomery product: field 0 Fr, 1 Fq; bits
+ * 8.. select the formulation (0 the library's product, 1 a 64-bit-accumulation
+ * variant, 2 squaring).  Returns products per second and the best kernel ms. */
 int nkr_b200_bench_mul(nkr_b200_ctx *ctx, int field, double *muls_per_s, double *ms);
 
 /* ---- setup ------------------------------------------------------------------ */

@@ -7,6 +7,7 @@
 #include <memory>
 #include <mutex>
 
+#include "../host/fr_host.hpp"
 #include "msm.cuh"
 #include "ntt.cuh"
 #include "ops.cuh"
@@ -285,9 +286,13 @@ static int msm_plain(nkr_b200_ctx *ctx, int group, const void *bases, const void
     DevBuf ds;
     NKR_TRY(ds.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
     if (n) NKR_CUDA(cudaMemcpyAsync(ds.p, scalars, n * 32, cudaMemcpyHostToDevice, st));
-    NKR_TRY(msm_run(b, s, ds.p, s.result.p, st));
-    NKR_CUDA(cudaMemcpyAsync(out, s.result.p, group == 1 ? 96 : 192, cudaMemcpyDeviceToHost, st));
+    NKR_TRY(msm_run(b, s, ds.p, s.acc.result.p, st));
+    NKR_CUDA(cudaMemcpyAsync(out, s.acc.result.p, group == 1 ? 96 : 192, cudaMemcpyDeviceToHost, st));
     NKR_CUDA(cudaStreamSynchronize(st));
+    if (group == 1)
+        host::normalize_g1(out);
+    else
+        host::normalize_g2(out);
     return NKR_B200_OK;
 }
 
@@ -310,9 +315,9 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     h->ctx = ctx;
     NKR_TRY(msm_bases_build(h->bases, group, bases, false, n, true, 0, false, ctx->stream));
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
-    NKR_CUDA(cudaEventCreate(&h->scratch.ev_acc[0]));
-    NKR_CUDA(cudaEventCreate(&h->scratch.ev_acc[1]));
-    h->scratch.timing = true;
+    NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[0]));
+    NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[1]));
+    h->scratch.acc.timing = true;
     NKR_TRY(h->scalars.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
     *out = h.release();
     return NKR_B200_OK;
@@ -343,9 +348,9 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
     NKR_CUDA(cudaEventCreate(&e0));
     NKR_CUDA(cudaEventCreate(&e1));
     NKR_CUDA(cudaEventRecord(e0, st));
-    const int s = msm_run(b->bases, b->scratch, src, b->scratch.result.p, st);
+    const int s = msm_run(b->bases, b->scratch, src, b->scratch.acc.result.p, st);
     NKR_CUDA(cudaEventRecord(e1, st));
-    NKR_CUDA(cudaMemcpyAsync(out, b->scratch.result.p, b->bases.group == 1 ? 96 : 192,
+    NKR_CUDA(cudaMemcpyAsync(out, b->scratch.acc.result.p, b->bases.group == 1 ? 96 : 192,
                              cudaMemcpyDeviceToHost, st));
     NKR_CUDA(cudaStreamSynchronize(st));
     float total = 0.f;
@@ -354,12 +359,16 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (s == NKR_B200_OK) {
+        if (b->bases.group == 1)
+            host::normalize_g1(out);
+        else
+            host::normalize_g2(out);
         b->last.total_ms = total;
-        NKR_CUDA(cudaEventElapsedTime(&b->last.acc_ms, b->scratch.ev_acc[0], b->scratch.ev_acc[1]));
+        NKR_CUDA(cudaEventElapsedTime(&b->last.acc_ms, b->scratch.acc.ev_acc[0], b->scratch.acc.ev_acc[1]));
         uint32_t entries = 0, tasks = 0;
         const uint32_t nb = b->bases.shape.nb;
-        NKR_CUDA(cudaMemcpy(&entries, b->scratch.offsets.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
-        NKR_CUDA(cudaMemcpy(&tasks, b->scratch.task_off.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
+        NKR_CUDA(cudaMemcpy(&entries, b->scratch.sort.offsets.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
+        tasks = uint32_t((uint64_t(entries) + b->bases.shape.k1 - 1) / b->bases.shape.k1);
         b->last.entries = entries;
         b->last.tasks = tasks;
         b->last.window_bits = uint32_t(b->bases.shape.c);
@@ -381,7 +390,7 @@ void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
     if (!b) return;
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
-    for (auto &e : b->scratch.ev_acc)
+    for (auto &e : b->scratch.acc.ev_acc)
         if (e) cudaEventDestroy(e);
     delete b;
 }

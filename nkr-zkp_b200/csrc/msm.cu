@@ -1,21 +1,15 @@
 // Pippenger MSM kernels (design notes in msm.cuh).
+//
+// The curve arithmetic here chains many field products per thread, so the
+// product is compiled out of line (one body per kernel) to keep the hot loops
+// resident in the instruction cache.
+#define NKR_FIELD_MUL_OUTLINE 1
 #include "msm.cuh"
 #include "scan.cuh"
 
 namespace nkr {
 
 namespace {
-
-template <int G>
-struct GroupField;
-template <>
-struct GroupField<1> {
-    using F = Fq;
-};
-template <>
-struct GroupField<2> {
-    using F = Fq2;
-};
 
 // --------------------------------------------------------------------------
 // signed digits
@@ -31,17 +25,17 @@ __device__ __forceinline__ uint32_t window_bits(const Fr &s, int off, int c)
     return uint32_t(w >> sh) & ((1u << c) - 1u);
 }
 
-// Walks the signed digits of one scalar; calls f(k, bucket_in_set, negative)
-// for every nonzero digit.  Digits: v = bits + carry; v > 2^(c-1) -> v - 2^c.
+// Walks the signed digits of one scalar; calls f(k, has, bucket_in_set, negative)
+// for every window.  Digits: v = bits + carry; v > 2^(c-1) -> v - 2^c.
 template <class Fn>
 __device__ __forceinline__ void for_each_digit(const Fr &s, int c, int W, Fn &&f)
 {
     uint32_t carry = 0;
     const uint32_t half = 1u << (c - 1), full = 1u << c;
     for (int k = 0; k < W; ++k) {
-        uint32_t v = window_bits(s, k * c, c) + carry;
-        bool has = false, negd = false;
-        uint32_t mag = 0;
+        const uint32_t v = window_bits(s, k * c, c) + carry;
+        bool has, negd = false;
+        uint32_t mag;
         if (v > half) {
             carry = 1;
             mag = full - v;
@@ -103,15 +97,6 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
     });
 }
 
-struct LoadTasks {
-    const uint32_t *counts;
-    uint32_t k1;
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const
-    {
-        return (counts[i] + k1 - 1) / k1;
-    }
-};
-
 // first index in a[0, n) with a[idx] > x (a nondecreasing)
 __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t *a, uint32_t n, uint32_t x)
 {
@@ -130,105 +115,226 @@ __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t *a, uint32_t 
 // bucket accumulation
 // --------------------------------------------------------------------------
 
+// Pieces of a bucket at level 1: the bucket's entries [off_b, off_b+1) are cut
+// by the fixed segments of K1 entries; a bucket inside one segment is complete,
+// otherwise it has one piece per segment it touches.  Piece k of bucket b lives
+// in partial slot 2 t (the segment's first run) or 2 t + 1 (its last run).
+struct Pieces {
+    uint32_t t0, count;
+    __device__ __forceinline__ uint64_t slot(const uint32_t off_b, uint32_t k1, uint32_t k) const
+    {
+        if (k == 0) return off_b == t0 * k1 ? 2ull * t0 : 2ull * t0 + 1;
+        return 2ull * (t0 + k);
+    }
+};
+
+__device__ __forceinline__ Pieces bucket_pieces(const uint32_t *offsets, uint32_t b, uint32_t k1)
+{
+    const uint32_t lo = offsets[b], hi = offsets[b + 1];
+    if (hi == lo) return {0, 0};
+    const uint32_t t0 = lo / k1, t1 = (hi - 1) / k1;
+    return {t0, t1 - t0 + 1};
+}
+
+// Groups of k2 pieces a bucket still has at a fix-up level whose inputs are
+// spaced `stride` pieces apart (zero once the bucket is complete).
+struct LoadLeaders {
+    const uint32_t *offsets;
+    uint32_t k1, stride, k2;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const
+    {
+        const Pieces pc = bucket_pieces(offsets, uint32_t(i), k1);
+        const uint32_t live = (pc.count + stride - 1) / stride;
+        return live > 1 ? (live + k2 - 1) / k2 : 0u;
+    }
+};
+
+// Level 1: thread t sums the fixed segment [t K1, (t+1) K1) of the sorted
+// entries, split into runs at bucket boundaries, so every lane of a warp does
+// the same number of mixed additions whatever the bucket sizes.  A run that is
+// a whole bucket is written to the bucket; the segment's first / last run, when
+// its bucket continues outside the segment, goes to partial slot 2t / 2t + 1.
 template <class F>
-__global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ task_off,
-                                                 const uint32_t *__restrict__ offsets,
+__global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
                                                  const uint32_t *__restrict__ entries,
                                                  const Affine<F> *__restrict__ pts, uint32_t nb,
-                                                 int k1, uint32_t *__restrict__ task_bucket,
-                                                 Xyzz<F> *__restrict__ partials,
+                                                 uint32_t k1, Xyzz<F> *__restrict__ partials,
                                                  Xyzz<F> *__restrict__ buckets)
 {
-    const uint32_t T1 = task_off[nb];
+    const uint32_t total = offsets[nb];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T1) return;
-    const uint32_t b = upper_bound_u32(task_off, nb + 1, t) - 1;
-    const uint32_t ts = task_off[b], te = task_off[b + 1];
-    const uint32_t beg = offsets[b] + (t - ts) * uint32_t(k1);
-    const uint32_t end = min(beg + uint32_t(k1), offsets[b + 1]);
+    const uint64_t beg64 = uint64_t(t) * k1;
+    if (beg64 >= total) return;
+    const uint32_t beg = uint32_t(beg64);
+    const uint32_t end = min(beg + k1, total);
+    uint32_t b = upper_bound_u32(offsets, nb + 1, beg) - 1; // offsets[b] <= beg < offsets[b + 1]
+    uint32_t bstart = offsets[b], bend = offsets[b + 1];
+    bool first = true;
     Xyzz<F> acc = Xyzz<F>::inf();
+    // one flat loop with the same trip count in every lane keeps the additions
+    // converged; the flush at a bucket boundary is a short divergent branch
     for (uint32_t j = beg; j < end; ++j) {
+        if (j == bend) {
+            if (bstart >= beg)
+                buckets[b] = acc; // the bucket started and ended inside the segment
+            else
+                partials[2ull * t] = acc; // first run, bucket began in an earlier segment
+            first = false;
+            acc = Xyzz<F>::inf();
+            // next nonempty bucket: usually adjacent, else search
+            ++b;
+            int steps = 0;
+            while (offsets[b + 1] <= j && steps < 8) {
+                ++b;
+                ++steps;
+            }
+            if (offsets[b + 1] <= j) b = upper_bound_u32(offsets, nb + 1, j) - 1;
+            bstart = offsets[b];
+            bend = offsets[b + 1];
+        }
         const uint32_t e = entries[j];
         Affine<F> p = pts[e & 0x7fffffffu];
         if (e >> 31) p = affine_neg(p);
         acc = xyzz_add_affine(acc, p);
     }
-    task_bucket[t] = b;
-    if (te - ts == 1)
+    if (bstart >= beg && bend <= end)
         buckets[b] = acc;
     else
-        partials[t] = acc;
+        partials[2ull * t + (first ? 0 : 1)] = acc;
 }
 
+// One thread per group of k2 pieces (spaced `stride` pieces apart) of one
+// bucket; the group's sum goes back into the group's first piece slot, or into
+// the bucket when it was the bucket's last group.
 template <class F>
-__global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ task_off, uint32_t nb,
-                                                 const uint32_t *__restrict__ task_bucket,
-                                                 Xyzz<F> *__restrict__ partials,
+__global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ offsets,
+                                                 const uint32_t *__restrict__ lead_off, uint32_t nb,
+                                                 uint32_t k1, Xyzz<F> *__restrict__ partials,
                                                  Xyzz<F> *__restrict__ buckets, uint32_t stride,
                                                  uint32_t k2)
 {
-    const uint32_t T1 = task_off[nb];
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T1) return;
-    const uint32_t b = task_bucket[t];
-    const uint32_t ts = task_off[b], te = task_off[b + 1];
-    const uint32_t cnt = te - ts;
-    if (cnt == 1) return;
-    const uint32_t r = t - ts;
-    const uint64_t group = uint64_t(stride) * k2;
-    if (r % group) return;
-    const uint32_t live = (cnt + stride - 1) / stride; // partials left from the previous level
-    if (live <= 1) return;
+    const uint32_t total = lead_off[nb];
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= total) return;
+    const uint32_t b = upper_bound_u32(lead_off, nb + 1, q) - 1;
+    const uint32_t j = q - lead_off[b];
+    const Pieces pc = bucket_pieces(offsets, b, k1);
+    const uint32_t off_b = offsets[b];
+    const uint32_t live = (pc.count + stride - 1) / stride;
+    const uint64_t r = uint64_t(j) * k2 * stride;
     Xyzz<F> acc = Xyzz<F>::inf();
     for (uint32_t m = 0; m < k2; ++m) {
-        const uint64_t idx = uint64_t(r) + uint64_t(m) * stride;
-        if (idx >= cnt) break;
-        acc = xyzz_add(acc, partials[ts + idx]);
+        const uint64_t idx = r + uint64_t(m) * stride;
+        if (idx >= pc.count) break;
+        acc = xyzz_add(acc, partials[pc.slot(off_b, k1, uint32_t(idx))]);
     }
     if (live <= k2)
         buckets[b] = acc;
     else
-        partials[t] = acc;
+        partials[pc.slot(off_b, k1, uint32_t(r))] = acc;
 }
 
 // --------------------------------------------------------------------------
 // bucket reduction: sum_b b * S_b per set, then + sum_b S_b
 // --------------------------------------------------------------------------
 
+// Work-efficient first level for large bucket sets: a thread takes L
+// consecutive buckets and forms T = sum_i i S_i and R = sum_i S_i by running
+// sums (2 additions per bucket), emitting one (A = T, R) item per L buckets
+// with unit L for the block levels that follow.
 template <class F>
-__global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<F> *__restrict__ a_in,
-                                                       const Xyzz<F> *__restrict__ r_in,
-                                                       uint32_t sets, uint32_t m, uint32_t L,
-                                                       int log2_unit, Xyzz<F> *__restrict__ a_out,
+__global__ void __launch_bounds__(128) k_reduce_chunk(const Xyzz<F> *__restrict__ r_in,
+                                                       uint64_t items, uint32_t L,
+                                                       Xyzz<F> *__restrict__ a_out,
                                                        Xyzz<F> *__restrict__ r_out)
 {
-    const uint32_t cps = m / L;
     const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= uint64_t(sets) * cps) return;
-    const uint64_t base = (t / cps) * m + (t % cps) * L;
-    Xyzz<F> run = Xyzz<F>::inf(), tri = Xyzz<F>::inf(), asum = Xyzz<F>::inf();
+    if (t * L >= items) return;
+    const uint64_t base = t * L;
+    Xyzz<F> run = Xyzz<F>::inf(), tri = Xyzz<F>::inf();
     for (int i = int(L) - 1; i >= 0; --i) {
         run = xyzz_add(run, r_in[base + i]);
         if (i > 0) tri = xyzz_add(tri, run);
-        if (a_in) asum = xyzz_add(asum, a_in[base + i]);
     }
-    for (int d = 0; d < log2_unit; ++d) tri = xyzz_dbl(tri);
-    a_out[t] = xyzz_add(tri, asum);
+    a_out[t] = tri;
     r_out[t] = run;
 }
 
-template <class F>
-__device__ __forceinline__ void store_jacobian_layout(const Affine<F> &a, F *out)
+// One level of the weighted sum: items carry (A_c, R_c) with
+// S = sum_c (A_c + c U R_c) (unit U = 2^log2_unit; level 0 is A = 0, R = the
+// buckets, U = 1).  A block takes BS consecutive
+// items c (padding with infinity), forms the suffix sums Suf_c = sum_{c' >= c} R_c'
+// with a Hillis-Steele scan in shared memory (log2 BS dependent additions),
+// then sum_c c R_c = sum_{c >= 1} Suf_c and sum_c A_c by tree sums, so a level
+// costs about 2 log2(BS) dependent additions instead of 2 BS.
+// Output per block: A' = sum A_c + U sum_c c R_c, R' = sum R_c.
+template <class F, int BS>
+__global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__ a_in,
+                                                      const Xyzz<F> *__restrict__ r_in,
+                                                      uint32_t m, int log2_unit,
+                                                      Xyzz<F> *__restrict__ a_out,
+                                                      Xyzz<F> *__restrict__ r_out)
 {
-    if (a.is_inf()) {
+    extern __shared__ uint8_t smem_raw[];
+    Xyzz<F> *buf0 = reinterpret_cast<Xyzz<F> *>(smem_raw);
+    Xyzz<F> *buf1 = buf0 + BS;
+    const uint32_t blocks_per_set = (m + BS - 1) / BS;
+    const uint32_t set = blockIdx.x / blocks_per_set;
+    const uint32_t blk = blockIdx.x % blocks_per_set;
+    const int i = threadIdx.x;
+    const uint64_t idx = uint64_t(blk) * BS + i;
+    const bool live = idx < m;
+    const uint64_t g = uint64_t(set) * m + idx;
+    Xyzz<F> v = live ? r_in[g] : Xyzz<F>::inf();
+    buf0[i] = v;
+    __syncthreads();
+    Xyzz<F> *cur = buf0, *nxt = buf1;
+    for (int d = 1; d < BS; d <<= 1) {
+        if (i + d < BS) v = xyzz_add(v, cur[i + d]);
+        nxt[i] = v;
+        __syncthreads();
+        Xyzz<F> *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    // v = Suf_i.  R' = Suf_0; weighted part = sum_{i >= 1} Suf_i; A part = sum A_i
+    const Xyzz<F> total = cur[0];
+    __syncthreads();
+    buf0[i] = i >= 1 ? v : Xyzz<F>::inf();
+    buf1[i] = (a_in && live) ? a_in[g] : Xyzz<F>::inf();
+    __syncthreads();
+    for (int s = BS / 2; s > 0; s >>= 1) {
+        if (i < s) {
+            buf0[i] = xyzz_add(buf0[i], buf0[i + s]);
+            buf1[i] = xyzz_add(buf1[i], buf1[i + s]);
+        }
+        __syncthreads();
+    }
+    if (i == 0) {
+        Xyzz<F> w = buf0[0];
+        for (int d = 0; d < log2_unit; ++d) w = xyzz_dbl(w);
+        const uint32_t o = set * blocks_per_set + blk;
+        a_out[o] = xyzz_add(w, buf1[0]);
+        r_out[o] = total;
+    }
+}
+
+// XYZZ -> libff Jacobian layout without inversion: with Z = ZZ ZZZ,
+// X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point.
+template <class F>
+__device__ __forceinline__ void store_jacobian(const Xyzz<F> &p, F *out)
+{
+    if (p.is_inf()) {
         out[0] = F::zero();
         out[1] = F::one();
         out[2] = F::zero();
-    } else {
-        out[0] = a.x;
-        out[1] = a.y;
-        out[2] = F::one();
+        return;
     }
+    const F zzz2 = sqr(p.zzz);
+    const F zz2 = sqr(p.zz);
+    out[0] = p.x * (p.zz * zzz2);
+    out[1] = p.y * (zz2 * p.zz * zzz2);
+    out[2] = p.zz * p.zzz;
 }
 
 template <class F>
@@ -239,9 +345,9 @@ __global__ void k_finalize(const Xyzz<F> *a, const Xyzz<F> *r, int sets, int c, 
     for (int k = sets - 1; k >= 0; --k) {
         if (k != sets - 1)
             for (int d = 0; d < c; ++d) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, xyzz_add(a[k], r[k]));
+        acc = xyzz_add(acc, a ? xyzz_add(a[k], r[k]) : r[k]);
     }
-    store_jacobian_layout(xyzz_to_affine(acc), out);
+    store_jacobian(acc, out);
 }
 
 // --------------------------------------------------------------------------
@@ -368,71 +474,67 @@ int build_windows_t(MsmBases &b, cudaStream_t st)
 }
 
 template <class F>
-int msm_run_t(const MsmBases &bs, MsmScratch &s, const void *scalars_dev, void *out_dev,
-              cudaStream_t st)
+int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
     const MsmShape &sh = bs.shape;
-    const uint64_t n = sh.n;
-    NKR_CUDA(cudaMemsetAsync(s.counts.p, 0, (sh.nb + 1) * 4, st));
-    NKR_CUDA(cudaMemsetAsync(s.buckets.p, 0, uint64_t(sh.nb) * sizeof(Xyzz<F>), st));
-    if (n) {
-        k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>(
-            static_cast<const Fr *>(scalars_dev), n, sh.c, sh.W, sh.folded, sh.B, s.canon.as<Fr>(),
-            s.counts.as<uint32_t>());
-        NKR_CHECK_LAUNCH();
-    }
-    NKR_TRY(scan_exclusive(LoadU32{s.counts.as<uint32_t>()}, sh.nb, s.offsets.as<uint32_t>(),
-                           s.scan_tmp.as<uint32_t>(), st));
-    NKR_TRY(scan_exclusive(LoadTasks{s.counts.as<uint32_t>(), uint32_t(sh.k1)}, sh.nb,
-                           s.task_off.as<uint32_t>(), s.scan_tmp.as<uint32_t>(), st));
-    NKR_CUDA(cudaMemcpyAsync(s.cursor.p, s.offsets.p, uint64_t(sh.nb) * 4,
-                             cudaMemcpyDeviceToDevice, st));
-    if (n) {
-        k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(s.canon.as<Fr>(), n, sh.c, sh.W, sh.folded,
-                                                      sh.B, s.cursor.as<uint32_t>(),
-                                                      s.entries.as<uint32_t>());
-        NKR_CHECK_LAUNCH();
-    }
-    const uint64_t tmax = sh.tasks_max();
-    const unsigned tb = blocks_for(tmax, 128);
-    if (s.timing) NKR_CUDA(cudaEventRecord(s.ev_acc[0], st));
-    k_acc_l1<F><<<tb, 128, 0, st>>>(s.task_off.as<uint32_t>(), s.offsets.as<uint32_t>(),
-                                    s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, sh.k1,
-                                    s.task_bucket.as<uint32_t>(), s.partials.as<Xyzz<F>>(),
-                                    s.buckets.as<Xyzz<F>>());
+    NKR_CUDA(cudaMemsetAsync(a.buckets.p, 0, uint64_t(sh.nb) * sizeof(Xyzz<F>), st));
+    const uint64_t segs = sh.segments_max();
+    const uint32_t *offsets = s.offsets.as<uint32_t>();
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[0], st));
+    k_acc_l1<F><<<blocks_for(segs, 128), 128, 0, st>>>(offsets, s.entries.as<uint32_t>(),
+                                                       bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
+                                                       a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
-    if (s.timing) NKR_CUDA(cudaEventRecord(s.ev_acc[1], st));
-    // fix-up levels until one task's fan-in covers the largest possible bucket
-    for (uint64_t stride = 1; stride < tmax; stride *= uint64_t(sh.k2)) {
-        k_acc_up<F><<<tb, 128, 0, st>>>(s.task_off.as<uint32_t>(), sh.nb,
-                                        s.task_bucket.as<uint32_t>(), s.partials.as<Xyzz<F>>(),
-                                        s.buckets.as<Xyzz<F>>(), uint32_t(stride), uint32_t(sh.k2));
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[1], st));
+    // fix-up levels: inputs spaced `stride` pieces apart, groups of k2; one
+    // bucket has at most segs + 1 pieces, all buckets at most 2 segs
+    const uint64_t k2 = uint64_t(sh.k2);
+    for (uint64_t stride = 1; stride < segs + 1; stride *= k2) {
+        NKR_TRY(scan_exclusive(LoadLeaders{offsets, uint32_t(sh.k1), uint32_t(stride), uint32_t(k2)},
+                               sh.nb, a.lead_off.as<uint32_t>(), a.scan_tmp.as<uint32_t>(), st));
+        const uint64_t bound = 2 * segs / (stride * k2) + sh.nb + 1;
+        k_acc_up<F><<<blocks_for(bound, 128), 128, 0, st>>>(offsets, a.lead_off.as<uint32_t>(), sh.nb,
+                                                            uint32_t(sh.k1), a.partials.as<Xyzz<F>>(),
+                                                            a.buckets.as<Xyzz<F>>(), uint32_t(stride),
+                                                            uint32_t(k2));
         NKR_CHECK_LAUNCH();
     }
     // bucket reduction levels
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     uint32_t m = sh.B;
     const Xyzz<F> *a_in = nullptr;
-    const Xyzz<F> *r_in = s.buckets.as<Xyzz<F>>();
-    Xyzz<F> *bufs_a[2] = {s.red_a.as<Xyzz<F>>(), s.red_a2.as<Xyzz<F>>()};
-    Xyzz<F> *bufs_r[2] = {s.red_r.as<Xyzz<F>>(), s.red_r2.as<Xyzz<F>>()};
+    const Xyzz<F> *r_in = a.buckets.as<Xyzz<F>>();
+    Xyzz<F> *bufs_a[2] = {a.red_a.as<Xyzz<F>>(), a.red_a2.as<Xyzz<F>>()};
+    Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
     int flip = 0, log2_unit = 0;
+    constexpr int BS = sizeof(F) == sizeof(Fq) ? 256 : 128; // G1: 256 buckets per block, G2: 128
+    constexpr int kLog2BS = BS == 256 ? 8 : 7;
+    const size_t smem = 2 * BS * sizeof(Xyzz<F>);
+    NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)));
+    if (m >= (1u << 16)) {
+        // large sets: one work-efficient pass of 16 buckets per thread first
+        constexpr uint32_t L = 16;
+        const uint64_t items = uint64_t(sets) * m;
+        k_reduce_chunk<F><<<blocks_for(items / L, 128), 128, 0, st>>>(r_in, items, L, bufs_a[0],
+                                                                      bufs_r[0]);
+        NKR_CHECK_LAUNCH();
+        a_in = bufs_a[0];
+        r_in = bufs_r[0];
+        flip = 1;
+        m /= L;
+        log2_unit = 4;
+    }
     while (m > 1) {
-        const uint32_t L = m >= 8 ? 8u : m;
-        const uint64_t threads = uint64_t(sets) * (m / L);
-        k_reduce_level<F><<<blocks_for(threads, 128), 128, 0, st>>>(
-            a_in, r_in, sets, m, L, log2_unit, bufs_a[flip], bufs_r[flip]);
+        const uint32_t per_set = (m + BS - 1) / BS;
+        k_reduce_block<F, BS><<<sets * per_set, BS, smem, st>>>(a_in, r_in, m, log2_unit, bufs_a[flip],
+                                                               bufs_r[flip]);
         NKR_CHECK_LAUNCH();
         a_in = bufs_a[flip];
         r_in = bufs_r[flip];
         flip ^= 1;
-        m /= L;
-        log2_unit += (L == 8 ? 3 : (L == 4 ? 2 : (L == 2 ? 1 : 0)));
-    }
-    if (a_in == nullptr) {
-        // a single bucket per set: weight 1 each
-        NKR_CUDA(cudaMemsetAsync(s.red_a.p, 0, uint64_t(sets) * sizeof(Xyzz<F>), st));
-        a_in = s.red_a.as<Xyzz<F>>();
+        m = per_set;
+        log2_unit += kLog2BS;
     }
     k_finalize<F><<<1, 32, 0, st>>>(a_in, r_in, int(sets), sh.c, static_cast<F *>(out_dev));
     NKR_CHECK_LAUNCH();
@@ -440,25 +542,20 @@ int msm_run_t(const MsmBases &bs, MsmScratch &s, const void *scalars_dev, void *
 }
 
 template <class F>
-int scratch_alloc_t(MsmScratch &s, const MsmShape &sh)
+int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
 {
-    const uint64_t tmax = sh.tasks_max();
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     const uint64_t red = uint64_t(sets) * (sh.B / 8 + 1);
-    NKR_TRY(s.canon.alloc(std::max<uint64_t>(sh.n, 1) * sizeof(Fr), "msm canonical scalars"));
-    NKR_TRY(s.counts.alloc((sh.nb + 1) * 4ull, "msm bucket counts"));
-    NKR_TRY(s.offsets.alloc((sh.nb + 1) * 4ull, "msm bucket offsets"));
-    NKR_TRY(s.cursor.alloc((sh.nb + 1) * 4ull, "msm scatter cursor"));
-    NKR_TRY(s.task_off.alloc((sh.nb + 1) * 4ull, "msm task offsets"));
-    NKR_TRY(s.entries.alloc(std::max<uint64_t>(sh.entries_max(), 1) * 4, "msm entries"));
-    NKR_TRY(s.task_bucket.alloc(tmax * 4, "msm task buckets"));
-    NKR_TRY(s.partials.alloc(tmax * sizeof(Xyzz<F>), "msm partial sums"));
-    NKR_TRY(s.buckets.alloc(uint64_t(sh.nb) * sizeof(Xyzz<F>), "msm buckets"));
-    NKR_TRY(s.red_a.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
-    NKR_TRY(s.red_r.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
-    NKR_TRY(s.red_a2.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
-    NKR_TRY(s.red_r2.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
-    NKR_TRY(s.scan_tmp.alloc(scan_scratch_words(sh.nb) * 4, "msm scan scratch"));
+    NKR_TRY(a.partials.alloc(2 * std::max<uint64_t>(sh.segments_max(), 1) * sizeof(Xyzz<F>),
+                             "msm partial sums"));
+    NKR_TRY(a.buckets.alloc(uint64_t(sh.nb) * sizeof(Xyzz<F>), "msm buckets"));
+    NKR_TRY(a.lead_off.alloc((sh.nb + 1) * 4ull, "msm fix-up offsets"));
+    NKR_TRY(a.red_a.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
+    NKR_TRY(a.red_r.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
+    NKR_TRY(a.red_a2.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
+    NKR_TRY(a.red_r2.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
+    NKR_TRY(a.scan_tmp.alloc(scan_scratch_words(sh.nb) * 4, "msm scan scratch"));
+    NKR_TRY(a.result.alloc(192, "msm result"));
     return NKR_B200_OK;
 }
 
@@ -472,16 +569,28 @@ MsmShape msm_shape(uint64_t n, bool folded, int group, int c_override)
     int lg = 0;
     while ((uint64_t(1) << lg) < n) ++lg;
     int c;
+    (void)group; // G1 and G2 share the shape so MSMs over the same scalars share one sort
     if (c_override > 0) {
         c = c_override;
     } else if (folded) {
-        c = lg - 4; // one bucket set: larger windows pay off
-        if (group == 2) c -= 1;
+        // One bucket set.  Cost model in point additions: n ceil(255 / c) mixed
+        // additions (10 products each) for the accumulation against about two
+        // full additions (14 products each) per bucket for the reduction.
+        double best = 1e300;
+        c = 8;
+        for (int cc = 8; cc <= 22; ++cc) {
+            const double cost = double(n) * ((255 + cc - 1) / cc) * 10.0 +
+                                double(uint64_t(1) << (cc - 1)) * 2.0 * 14.0;
+            if (cost < best) {
+                best = cost;
+                c = cc;
+            }
+        }
     } else {
         c = lg - 5;
     }
     if (c < 4) c = 4;
-    if (c > 20) c = 20;
+    if (c > 22) c = 22;
     sh.c = c;
     sh.W = (255 + c - 1) / c;
     sh.B = 1u << (c - 1);
@@ -536,18 +645,62 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
     return NKR_B200_OK;
 }
 
+int msm_sort_alloc(MsmSort &s, const MsmShape &sh)
+{
+    NKR_TRY(s.canon.alloc(std::max<uint64_t>(sh.n, 1) * sizeof(Fr), "msm canonical scalars"));
+    NKR_TRY(s.counts.alloc((sh.nb + 1) * 4ull, "msm bucket counts"));
+    NKR_TRY(s.offsets.alloc((sh.nb + 1) * 4ull, "msm bucket offsets"));
+    NKR_TRY(s.cursor.alloc((sh.nb + 1) * 4ull, "msm scatter cursor"));
+    NKR_TRY(s.entries.alloc(std::max<uint64_t>(sh.entries_max(), 1) * 4, "msm entries"));
+    NKR_TRY(s.scan_tmp.alloc(scan_scratch_words(sh.nb) * 4, "msm scan scratch"));
+    return NKR_B200_OK;
+}
+
+int msm_acc_alloc(MsmAcc &a, int group, const MsmShape &sh)
+{
+    return group == 1 ? acc_alloc_t<Fq>(a, sh) : acc_alloc_t<Fq2>(a, sh);
+}
+
 int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape)
 {
-    NKR_TRY(group == 1 ? scratch_alloc_t<Fq>(s, shape) : scratch_alloc_t<Fq2>(s, shape));
-    NKR_TRY(s.result.alloc(192, "msm result"));
+    NKR_TRY(msm_sort_alloc(s.sort, shape));
+    NKR_TRY(msm_acc_alloc(s.acc, group, shape));
     return NKR_B200_OK;
+}
+
+int msm_sort_run(const MsmShape &sh, MsmSort &s, const void *scalars_dev, cudaStream_t st)
+{
+    const uint64_t n = sh.n;
+    NKR_CUDA(cudaMemsetAsync(s.counts.p, 0, (sh.nb + 1) * 4, st));
+    if (n) {
+        k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>(
+            static_cast<const Fr *>(scalars_dev), n, sh.c, sh.W, sh.folded, sh.B, s.canon.as<Fr>(),
+            s.counts.as<uint32_t>());
+        NKR_CHECK_LAUNCH();
+    }
+    NKR_TRY(scan_exclusive(LoadU32{s.counts.as<uint32_t>()}, sh.nb, s.offsets.as<uint32_t>(),
+                           s.scan_tmp.as<uint32_t>(), st));
+    NKR_CUDA(cudaMemcpyAsync(s.cursor.p, s.offsets.p, uint64_t(sh.nb) * 4, cudaMemcpyDeviceToDevice,
+                             st));
+    if (n) {
+        k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(s.canon.as<Fr>(), n, sh.c, sh.W, sh.folded, sh.B,
+                                                      s.cursor.as<uint32_t>(),
+                                                      s.entries.as<uint32_t>());
+        NKR_CHECK_LAUNCH();
+    }
+    return NKR_B200_OK;
+}
+
+int msm_acc_run(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    return b.group == 1 ? acc_run_t<Fq>(b, s, a, out_dev, st) : acc_run_t<Fq2>(b, s, a, out_dev, st);
 }
 
 int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out_dev,
             cudaStream_t st)
 {
-    return b.group == 1 ? msm_run_t<Fq>(b, s, scalars_dev, out_dev, st)
-                        : msm_run_t<Fq2>(b, s, scalars_dev, out_dev, st);
+    NKR_TRY(msm_sort_run(b.shape, s.sort, scalars_dev, st));
+    return msm_acc_run(b, s.sort, s.acc, out_dev, st);
 }
 
 } // namespace nkr

@@ -7,21 +7,31 @@
 // correct bucket order is bit-exact after affine normalisation.
 //
 // Steps (all on the device, no host round trip):
-//  1. digits: each scalar leaves Montgomery form and is cut into W signed c-bit
+//  1. sort: each scalar leaves Montgomery form and is cut into W signed c-bit
 //     digits d in [-2^(c-1), 2^(c-1)]; bucket |d| - 1 receives the point
-//     (negated when d < 0).  Counts are histogrammed with warp-aggregated atomics.
-//  2. counting sort: exclusive scans give bucket offsets and, per bucket,
-//     ceil(count / K1) accumulation tasks; a scatter writes (point, sign) entries.
-//  3. accumulation: one thread per task sums up to K1 affine points into an XYZZ
-//     accumulator (mixed add 8M + 2S, with the doubling branch).  Buckets split
-//     over several tasks are finished by in-place tree levels of fan-in K2, so a
-//     bucket holding a large share of all points (repeated or small scalars)
-//     costs O(log n) sequential adds instead of O(n).
-//  4. bucket reduction: sum_b (b + 1) S_b by chunked running sums in log levels.
-//  5. windows: with resident "folded" bases the W windows share one bucket set
-//     because the bases hold the copies 2^(c k) P_i (built once at prepare, HBM
-//     is large); otherwise each window has its own set and a Horner pass combines
-//     them.
+//     (negated when d < 0).  Counts are histogrammed with warp-aggregated
+//     atomics, an exclusive scan gives bucket offsets, and a scatter writes
+//     (point, sign) entries in bucket order.  The sort depends only on the scalars and the
+//     window shape, so MSMs over the same scalars share one sort (the three G1
+//     witness MSMs of a prove; the reference shares it too, bucket.cuh:50-141).
+//  2. accumulation: thread t sums the fixed segment of K1 sorted entries
+//     [t K1, (t+1) K1) into XYZZ accumulators (mixed add 8M + 2S, with the
+//     doubling branch), one run per bucket it crosses, so all lanes do equal
+//     work whatever the bucket sizes.  A bucket spread over several segments
+//     leaves one partial per segment and is finished by fix-up levels of fan-in
+//     K2: each level scans, per bucket, how many groups of K2 pieces remain and
+//     gives every group its own thread, so a bucket holding a large share of all
+//     points (repeated or small scalars) costs O(log n) sequential additions.
+//  3. bucket reduction: sum_b (b + 1) S_b in levels of 256 (G1) / 128 (G2)
+//     items per block: a shared-memory suffix scan and tree sums make a level
+//     about 2 log2(block) dependent additions deep.
+//  4. windows: with resident "folded" bases the W windows share one bucket set
+//     because the bases hold the copies 2^(c k) P_i (built once at prepare; HBM
+//     is large); otherwise each window has its own set and a Horner pass
+//     combines them.
+//  5. output: Jacobian coordinates in the libff layout (X, Y, Z) with an
+//     arbitrary Z -- no device inversion on the critical path; the host
+//     normalises the few result points.
 #pragma once
 
 #include <cstdint>
@@ -38,26 +48,44 @@ struct MsmShape {
     bool folded = false;
     uint32_t B = 0;  // buckets per set: 2^(c-1)
     uint32_t nb = 0; // total buckets: folded ? B : W * B
-    int k1 = 32;     // points per accumulation task
-    int k2 = 8;      // fan-in of the fix-up levels
+    int k1 = 32;     // entries per level-1 segment (mixed additions per thread)
+    int k2 = 16;     // fan-in of the fix-up levels
     uint64_t entries_max() const { return uint64_t(W) * n; }
-    uint64_t tasks_max() const { return (entries_max() + k1 - 1) / k1 + nb; }
+    uint64_t segments_max() const { return (entries_max() + k1 - 1) / k1; }
+    bool same_sort(const MsmShape &o) const
+    {
+        return n == o.n && c == o.c && W == o.W && folded == o.folded && k1 == o.k1;
+    }
 };
 
 MsmShape msm_shape(uint64_t n, bool folded, int group, int c_override = 0);
 
-// Per-MSM device scratch, sized for a shape and reusable across calls.
-struct MsmScratch {
-    DevBuf canon, counts, offsets, cursor, task_off, entries, task_bucket, partials, buckets;
-    DevBuf red_a, red_r, red_a2, red_r2, scan_tmp, result;
-    bool timing = false;            // record events around the level-1 accumulation kernel
+// Digit sort of one scalar vector: bucket offsets and entries in bucket order.
+struct MsmSort {
+    DevBuf canon, counts, offsets, cursor, entries, scan_tmp;
+    size_t device_bytes() const
+    {
+        return canon.bytes + counts.bytes + offsets.bytes + cursor.bytes + entries.bytes +
+               scan_tmp.bytes;
+    }
+};
+
+// Accumulation state of one MSM (partials, buckets, reduction levels, result).
+struct MsmAcc {
+    DevBuf partials, buckets, lead_off, red_a, red_r, red_a2, red_r2, scan_tmp, result;
+    bool timing = false; // record events around the level-1 accumulation kernel
     cudaEvent_t ev_acc[2] = {nullptr, nullptr};
     size_t device_bytes() const
     {
-        return canon.bytes + counts.bytes + offsets.bytes + cursor.bytes + task_off.bytes +
-               entries.bytes + task_bucket.bytes + partials.bytes + buckets.bytes + red_a.bytes +
-               red_r.bytes + red_a2.bytes + red_r2.bytes + scan_tmp.bytes + result.bytes;
+        return partials.bytes + buckets.bytes + lead_off.bytes + red_a.bytes + red_r.bytes +
+               red_a2.bytes + red_r2.bytes + scan_tmp.bytes + result.bytes;
     }
+};
+
+struct MsmScratch {
+    MsmSort sort;
+    MsmAcc acc;
+    size_t device_bytes() const { return sort.device_bytes() + acc.device_bytes(); }
 };
 
 // Resident bases for one MSM: affine points, folded into W window copies when
@@ -79,10 +107,16 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
 // Normalise n libff-layout Jacobian points (device) into affine (device).
 int jacobian_to_affine(int group, const void *jac, void *aff, uint64_t n, cudaStream_t st);
 
+int msm_sort_alloc(MsmSort &s, const MsmShape &shape);
+int msm_acc_alloc(MsmAcc &a, int group, const MsmShape &shape);
 int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape);
 
-// Run one MSM: scalars Fr[n] (Montgomery, device).  The affine result is written
-// to out_dev in libff Jacobian layout (Z = 1, or (0, 1, 0) for infinity).
+// Sort the scalars Fr[n] (Montgomery, device) for the shape.
+int msm_sort_run(const MsmShape &shape, MsmSort &s, const void *scalars_dev, cudaStream_t st);
+// Accumulate / reduce with a finished sort of the same shape.  The result is
+// written to out_dev in libff Jacobian layout with an arbitrary Z (or Z = 0 for
+// infinity); normalise on the host (host/fr_host.hpp normalize_g1 / _g2).
+int msm_acc_run(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st);
 int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out_dev,
             cudaStream_t st);
 

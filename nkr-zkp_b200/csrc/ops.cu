@@ -87,22 +87,42 @@ __global__ void k_group_op(int op, const F *a, const F *b, F *out, uint64_t n)
 }
 
 // Each thread runs 4 independent product chains; the result is stored so the
-// work cannot be eliminated.
+// work cannot be eliminated.  variant 0: operator* (64-bit accumulation CIOS),
+// 1: mont_mul_cc (PTX carry-chain CIOS), 2: squaring.
 constexpr int kBenchIters = 256;
-template <class P>
+template <class P, int V>
 __global__ void __launch_bounds__(256) k_bench_mul(const Fp<P> *seed, Fp<P> *sink)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     Fp<P> a = seed[i & 255], b = seed[(i + 1) & 255], c = seed[(i + 2) & 255], d = seed[(i + 3) & 255];
     const Fp<P> m = seed[(i + 7) & 255];
     for (int k = 0; k < kBenchIters; ++k) {
-        a = a * m;
-        b = b * m;
-        c = c * m;
-        d = d * m;
+        if (V == 1) {
+            a = mont_mul_cc(a, m);
+            b = mont_mul_cc(b, m);
+            c = mont_mul_cc(c, m);
+            d = mont_mul_cc(d, m);
+        } else if (V == 2) {
+            a = sqr(a);
+            b = sqr(b);
+            c = sqr(c);
+            d = sqr(d);
+        } else {
+            a = a * m;
+            b = b * m;
+            c = c * m;
+            d = d * m;
+        }
     }
     const Fp<P> r = a + b + c + d;
     if (r.v[0] == 0x12345678u) sink[i] = r;
+}
+
+template <class P>
+__global__ void k_check_wide(const Fp<P> *a, const Fp<P> *b, uint32_t *bad, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && mont_mul_cc(a[i], b[i]) != a[i] * b[i]) atomicAdd(bad, 1u);
 }
 
 } // namespace
@@ -166,12 +186,32 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
     NKR_CUDA(cudaEventCreate(&e0));
     NKR_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
+    const int variant = field >> 8;
+    field &= 0xff;
+    if (variant == 1) {
+        // the alternative product must agree with operator* before it is timed
+        DevBuf bad;
+        NKR_TRY(bad.alloc(4, "bench check"));
+        NKR_CUDA(cudaMemsetAsync(bad.p, 0, 4, st));
+        k_check_wide<FqParams><<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1, bad.as<uint32_t>(),
+                                                   255);
+        NKR_CHECK_LAUNCH();
+        uint32_t nbad = 0;
+        NKR_CUDA(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, st));
+        NKR_CUDA(cudaStreamSynchronize(st));
+        NKR_REQUIRE(nbad == 0, "carry-chain product disagrees on %u inputs", nbad);
+    }
     for (int rep = 0; rep < 4; ++rep) {
         NKR_CUDA(cudaEventRecord(e0, st));
-        if (field == 0)
-            k_bench_mul<FrParams><<<blocks, 256, 0, st>>>(seed.as<Fr>(), sink.as<Fr>());
+        if (field == 0 && variant == 0)
+            k_bench_mul<FrParams, 0><<<blocks, 256, 0, st>>>(seed.as<Fr>(), sink.as<Fr>());
+        else if (variant == 0)
+            k_bench_mul<FqParams, 0><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+        else if (variant == 1)
+            k_bench_mul<FqParams, 1><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         else
-            k_bench_mul<FqParams><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+            k_bench_mul<FqParams, 2><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+        NKR_CHECK_LAUNCH();
         NKR_CUDA(cudaEventRecord(e1, st));
         NKR_CUDA(cudaEventSynchronize(e1));
         float t;

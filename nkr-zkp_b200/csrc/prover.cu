@@ -1,7 +1,10 @@
 // Groth16 prepare / prove / blind on one B200 (design notes in prover.cuh).
+// The blinding kernel chains scalar multiplications: out-of-line products.
+#define NKR_FIELD_MUL_OUTLINE 1
 #include <cstring>
 #include <vector>
 
+#include "../host/fr_host.hpp"
 #include "prover.cuh"
 
 namespace nkr {
@@ -78,6 +81,17 @@ __global__ void k_blind(const uint8_t *pk_const, const uint8_t *raw, const Fr *r
     store_libff(C, reinterpret_cast<Fq *>(out + 288));
 }
 
+} // namespace
+
+void normalize_raw(void *raw576)
+{
+    uint8_t *o = static_cast<uint8_t *>(raw576);
+    for (int i = 0; i < 4; ++i) host::normalize_g1(o + 96 * i);
+    host::normalize_g2(o + 384);
+}
+
+namespace {
+
 int check_witness_ptr(const void *p, cudaMemoryType *type)
 {
     cudaPointerAttributes attr{};
@@ -106,10 +120,15 @@ int prove_issue(nkr_b200_key *key, bool timed)
     NKR_TRY(spmv_multi(mats, 3, z, ys, s0));
     NKR_CUDA(cudaEventRecord(key->ev_z, s0));
     if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[1], s0));
-    // witness MSMs on their own streams, overlapping the H chain
-    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) {
-        NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_z, 0));
-        NKR_TRY(msm_run(key->bases[k], key->scratch[k], z, out + kOutOffset[k], key->st[k]));
+    // witness MSMs on their own streams, overlapping the H chain; one digit sort
+    // of z serves all four (same scalars, same window shape)
+    cudaStream_t sa = key->st[kMsmA];
+    NKR_CUDA(cudaStreamWaitEvent(sa, key->ev_z, 0));
+    NKR_TRY(msm_sort_run(key->bases[kMsmA].shape, key->sort_z, z, sa));
+    NKR_CUDA(cudaEventRecord(key->ev_sorted, sa));
+    for (int k : {kMsmB2, kMsmA, kMsmB1, kMsmL}) {
+        if (k != kMsmA) NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_sorted, 0));
+        NKR_TRY(msm_acc_run(key->bases[k], key->sort_z, key->acc[k], out + kOutOffset[k], key->st[k]));
         NKR_CUDA(cudaEventRecord(key->ev_done[k], key->st[k]));
     }
     // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
@@ -122,7 +141,8 @@ int prove_issue(nkr_b200_key *key, bool timed)
     NKR_TRY(fr_quotient_pointwise(az, bz, cz, h, rows, cst + kConstZinv, s0));
     NKR_TRY(ntt_dif(T, h, true, nullptr, T.t2.as<Fr>(), nullptr, s0));
     if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[2], s0));
-    NKR_TRY(msm_run(key->bases[kMsmH], key->scratch[kMsmH], h, out + kOutOffset[kMsmH], s0));
+    NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, key->sort_h, h, s0));
+    NKR_TRY(msm_acc_run(key->bases[kMsmH], key->sort_h, key->acc[kMsmH], out + kOutOffset[kMsmH], s0));
     if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[3], s0));
     for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2})
         NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
@@ -169,7 +189,8 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
             return fail(NKR_B200_ECUDA);
         }
     }
-    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess) {
+    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&key->ev_sorted, cudaEventDisableTiming) != cudaSuccess) {
         set_error("event creation failed");
         return fail(NKR_B200_ECUDA);
     }
@@ -189,8 +210,15 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
     NKR_PREP(msm_bases_build(key->bases[kMsmL], 1, pk->l_query, false, c->cols, true, 0, false, st));
     NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, 0, true, st));
     NKR_PREP(msm_bases_build(key->bases[kMsmB2], 2, pk->b_g2_query, false, c->cols, true, 0, false, st));
+    for (int k : {kMsmB1, kMsmL, kMsmB2})
+        if (!key->bases[k].shape.same_sort(key->bases[kMsmA].shape)) {
+            set_error("witness MSM shapes differ; the shared digit sort needs one shape");
+            return fail(NKR_B200_EINVAL);
+        }
+    NKR_PREP(msm_sort_alloc(key->sort_z, key->bases[kMsmA].shape));
+    NKR_PREP(msm_sort_alloc(key->sort_h, key->bases[kMsmH].shape));
     for (int k = 0; k < kNumMsm; ++k)
-        NKR_PREP(msm_scratch_alloc(key->scratch[k], key->bases[k].group, key->bases[k].shape));
+        NKR_PREP(msm_acc_alloc(key->acc[k], key->bases[k].group, key->bases[k].shape));
     NKR_PREP(key->z.alloc(c->cols * 32, "witness"));
     NKR_PREP(key->az.alloc(c->rows * 32, "az"));
     NKR_PREP(key->bz.alloc(c->rows * 32, "bz"));
@@ -248,6 +276,7 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     NKR_TRY(prove_issue(key, true));
     NKR_CUDA(cudaMemcpyAsync(key->pinned_out, key->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
     NKR_CUDA(cudaStreamSynchronize(s0));
+    normalize_raw(key->pinned_out);
     const uint8_t *o = static_cast<const uint8_t *>(key->pinned_out);
     std::memcpy(res->ar, o + 0, 96);
     std::memcpy(res->bs1, o + 96, 96);
@@ -358,6 +387,7 @@ int key_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int
         if (!pinned[i]) continue;
         cudaStreamSynchronize(keys[i]->st[kMsmH]);
         if (status == NKR_B200_OK) {
+            normalize_raw(pinned[i]);
             const uint8_t *o = static_cast<const uint8_t *>(pinned[i]);
             std::memcpy(out[i].ar, o, 96);
             std::memcpy(out[i].bs1, o + 96, 96);
@@ -390,6 +420,7 @@ void nkr_b200_key_free(nkr_b200_key *key)
         if (key->ev_done[k]) cudaEventDestroy(key->ev_done[k]);
     }
     if (key->ev_z) cudaEventDestroy(key->ev_z);
+    if (key->ev_sorted) cudaEventDestroy(key->ev_sorted);
     for (auto e : key->ev_t)
         if (e) cudaEventDestroy(e);
     if (key->pinned_out) cudaFreeHost(key->pinned_out);
@@ -405,7 +436,7 @@ uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
                  key->blind_io.bytes;
     for (int k = 0; k < 3; ++k)
         b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].values.bytes;
-    for (int k = 0; k < nkr::kNumMsm; ++k)
-        b += key->bases[k].device_bytes() + key->scratch[k].device_bytes();
+    for (int k = 0; k < nkr::kNumMsm; ++k) b += key->bases[k].device_bytes() + key->acc[k].device_bytes();
+    b += key->sort_z.device_bytes() + key->sort_h.device_bytes();
     return b;
 }

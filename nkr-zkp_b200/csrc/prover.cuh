@@ -36,13 +36,15 @@ struct nkr_b200_key {
     nkr::CsrDevice mat[3];
     nkr::NttTables ntt;
     nkr::MsmBases bases[nkr::kNumMsm];
-    nkr::MsmScratch scratch[nkr::kNumMsm];
+    nkr::MsmSort sort_z;               // digit sort of the witness, shared by the 4 witness MSMs
+    nkr::MsmSort sort_h;               // digit sort of H
+    nkr::MsmAcc acc[nkr::kNumMsm];
     nkr::DevBuf z, az, bz, cz, h;
     nkr::DevBuf out;      // 4 G1 + 1 G2 results, libff Jacobian layout (96 * 4 + 192 B)
     nkr::DevBuf pk_const; // alpha_g1, beta_g1, delta_g1 (G1 affine) and beta_g2, delta_g2 (G2 affine)
     nkr::DevBuf blind_io; // r, s in; proof out
     cudaStream_t st[nkr::kNumMsm] = {};
-    cudaEvent_t ev_z = nullptr, ev_done[nkr::kNumMsm] = {};
+    cudaEvent_t ev_z = nullptr, ev_sorted = nullptr, ev_done[nkr::kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
     void *pinned_in = nullptr;  // witness staging (cols * 32 B)
     void *pinned_out = nullptr; // results staging (576 B + proof)
@@ -53,7 +55,11 @@ struct nkr_b200_key {
 namespace nkr {
 
 // Issue one full prove on the key's streams, witness already in key->z.
-// Results land in key->out (device).  No host synchronisation.
+// Results land in key->out (device, Jacobian with arbitrary Z).  No host
+// synchronisation.
 int prove_issue(nkr_b200_key *key, bool timed);
+
+// Affine-normalise the 4 G1 + 1 G2 result points (576 B, libff layout) in place.
+void normalize_raw(void *raw576);
 
 } // namespace nkr

@@ -403,6 +403,36 @@ def ref_available():
     return os.path.exists(REF_PATH)
 
 
+DROPIN_PATH = os.path.join(HERE, "_ref", "libnkr_ref_b200.so")
+
+
+class RefDropIn:
+    """The reference's Groth16 code driving the B200 backend through its Backend
+    interface (oracle/ref_dropin.cpp + nkr-zkp_b200/integration/b200_backend.cpp)."""
+
+    def __init__(self):
+        if not os.path.exists(DROPIN_PATH):
+            raise FileNotFoundError(f"{DROPIN_PATH} missing; run `make -C oracle dropin`")
+        self.lib = ctypes.CDLL(DROPIN_PATH)
+        self.lib.dropin_last_error.restype = ctypes.c_char_p
+
+    def prove_verify(self, r1cs, pk_path, vk_path, witness, gpu_setup=False):
+        c = Oracle._circuit(None, r1cs)
+        verified, raw_equal = ctypes.c_int(-1), ctypes.c_int(-1)
+        name = ctypes.create_string_buffer(16)
+        w = _arr(witness)
+        rc = self.lib.dropin_prove_verify(ctypes.byref(c), str(pk_path).encode(), str(vk_path).encode(),
+                                          _p(w), ctypes.c_int(1 if gpu_setup else 0),
+                                          ctypes.byref(verified), ctypes.byref(raw_equal), name)
+        if rc != 0:
+            raise RuntimeError(self.lib.dropin_last_error().decode())
+        return bool(verified.value), bool(raw_equal.value), name.value.decode()
+
+
+def dropin_available():
+    return os.path.exists(DROPIN_PATH)
+
+
 # ---------------------------------------------------------------------------
 # BinaryArchive ("LKZ1", version 1) artifacts
 # ---------------------------------------------------------------------------
