@@ -47,6 +47,7 @@ WORKLOADS = {
 }
 METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
 REF_SAMPLE = ("poseidon", 128, 2)  # 2^16 constraints
+TRAFFIC_PER_ENTRY = (390.744064e6 + 48.899328e6) / 3373063  # k_acc_l1<Fq>, 2^18 capture
 
 
 def _dist():
@@ -331,6 +332,9 @@ def run_b200(args):
         # plus the task bucket ids and bucket / partial writes (128 B each)
         algo_bytes = st["entries"] * (64 + 4) + st["tasks"] * 2 * 128
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        # DRAM bytes per entry from an ncu capture of this kernel at 2^18 (read + write
+        # 439.6 MB over 3,373,063 entries), scaled to this launch's entries
+        traffic = round(st["entries"] * TRAFFIC_PER_ENTRY)
         roof = {"bound": "int", "kernel": "k_acc_l1<Fq> (G1 bucket accumulation)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),
                 "unit": "G Fq-mul/s", "frac": round(achieved / muls_peak, 3),
@@ -344,7 +348,9 @@ def run_b200(args):
                         "peak": hbm_peak, "unit": "GB/s",
                         "frac": round(algo_bytes / (acc_ms * 1e-3) / 1e9 / hbm_peak, 4),
                         "algorithmic_bytes": algo_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
-                "traffic": None}
+                "traffic": traffic, "traffic_unit": "bytes per launch",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 2^18, "
+                                  "130.3 B per entry, scaled by entries"}
         mb.free()
 
     # ---- CPU baseline (rank 0, N = 1 only) --------------------------------------
