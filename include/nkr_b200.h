@@ -139,6 +139,19 @@ int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses
  * libfqfft basic_radix2_domain.tcc:40-112. */
 int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n);
 
+/* The same five domain ops on DEVICE buffers, allocating no device memory.  No
+ * counterpart in the reference: it serves callers that cannot allocate (their own
+ * pool already holds the device's memory, or cudaFree's device-wide wait would
+ * stall their other streams).  in and out (may be equal) hold n Fr values on
+ * `device`; stream is a cudaStream_t (NULL = the default stream).  The call only
+ * enqueues work: synchronise the stream before reading out.  Scratch is one fixed
+ * array inside the library, shared by all calls on a device: n is limited to
+ * 2^16 (larger n returns NKR_B200_EINVAL), and two calls in flight at once on
+ * different streams or threads race.  The first call on a device builds the
+ * array's tables and waits for `stream`; make it before capturing any stream. */
+int nkr_b200_ntt_noalloc(int device, int op, const void *in, void *out, uint64_t n,
+                         void *stream);
+
 /* CSR SpMV over Fr: y = M z (host buffers).  Replaces
  * sparse_matrix_vector_multiplication (backends/cuda/include/spmvm/spmvm.cuh:12-30). */
 int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_t *row_ptr,

@@ -294,4 +294,48 @@ int fr_quotient_pointwise(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_t
     return NKR_B200_OK;
 }
 
+int ntt_constants_into(int logn, Fr *consts, cudaStream_t st)
+{
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT domain 2^%d outside [2, 2^28]", logn);
+    k_ntt_constants<<<1, 32, 0, st>>>(logn, consts);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int fr_powers_into(const Fr *base, Fr *out, uint64_t m, cudaStream_t st)
+{
+    k_powers<<<blocks_for((m + kPowRun - 1) / kPowRun, 128), 128, 0, st>>>(base, out, m);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int ntt_stage_twiddles_into(const Fr *pw, Fr *tw, int logn, cudaStream_t st)
+{
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT domain 2^%d outside [2, 2^28]", logn);
+    k_stage_twiddles<<<blocks_for(uint64_t(1) << logn, 256), 256, 0, st>>>(pw, tw, logn);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int ntt_dit_raw(int logn, const Fr *tw, Fr *data, const Fr *pre, const Fr *post,
+                const Fr *post_const, cudaStream_t st)
+{
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT domain 2^%d outside [2, 2^28]", logn);
+    int ts[4];
+    const int np = pass_plan(logn, ts);
+    const uint64_t n = uint64_t(1) << logn;
+    int s_lo = 0;
+    for (int p = 0; p < np; ++p) {
+        const int t = ts[p];
+        const int G = 1 << t;
+        const unsigned threads = G >= 64 ? unsigned(G / 2) : 32u;
+        k_ntt_pass<false><<<unsigned(n >> t), threads, G * sizeof(Fr), st>>>(
+            data, s_lo, t, tw, p == 0 ? pre : nullptr, p == np - 1 ? post : nullptr,
+            p == np - 1 ? post_const : nullptr);
+        NKR_CHECK_LAUNCH();
+        s_lo += t;
+    }
+    return NKR_B200_OK;
+}
+
 } // namespace nkr

@@ -64,4 +64,15 @@ int fr_scale_const(Fr *data, uint64_t n, const Fr *c, cudaStream_t st);
 int fr_quotient_pointwise(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_t n,
                           const Fr *zinv, cudaStream_t st);
 
+// Table pieces and the DIT transform over caller-owned device memory (nothing is
+// allocated; used by the allocation-free entry point).  The stage twiddle table
+// tw[2^s + k] = w_{2^(s+1)}^k does not depend on N, so one table built for 2^L
+// serves every domain 2^logn with logn <= L.
+int ntt_constants_into(int logn, Fr *consts /* Fr[8], layout of NttTables::consts */,
+                       cudaStream_t st);
+int fr_powers_into(const Fr *base, Fr *out, uint64_t m, cudaStream_t st); // out[i] = base^i
+int ntt_stage_twiddles_into(const Fr *pw /* w_N^i, i < N/2 */, Fr *tw, int logn, cudaStream_t st);
+int ntt_dit_raw(int logn, const Fr *tw, Fr *data, const Fr *pre, const Fr *post,
+                const Fr *post_const, cudaStream_t st);
+
 } // namespace nkr

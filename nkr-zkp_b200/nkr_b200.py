@@ -82,6 +82,7 @@ _SIGS = {
     "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
                                             ctypes.POINTER(RawProofC)]),
     "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
+    "nkr_b200_ntt_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _U64, _VP]),
     "nkr_b200_spmv": (ctypes.c_int, [_VP, _U64, _U64, _VP, _VP, _VP, _VP, _VP]),
     "nkr_b200_msm_g1": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
     "nkr_b200_msm_g2": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
@@ -201,6 +202,15 @@ def poseidon_hash2(left, right):
     out = np.zeros(4, np.uint64)
     _check(_lib.nkr_b200_poseidon_hash2(_ptr(_fr(left)), _ptr(_fr(right)), _ptr(out)), "poseidon")
     return out
+
+
+NTT_NOALLOC_MAX = 1 << 16
+
+
+def ntt_noalloc(device, op, in_ptr, out_ptr, n, stream_ptr=0):
+    """nkr_b200_ntt_noalloc on device pointers (enqueued on stream_ptr, not waited for)."""
+    _check(_lib.nkr_b200_ntt_noalloc(device, op, in_ptr, out_ptr, n, stream_ptr or None),
+           f"ntt_noalloc op {op}")
 
 
 def poseidon_parameters():
