@@ -313,7 +313,7 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     NKR_REQUIRE(out && (n == 0 || bases), "null argument");
     auto h = std::make_unique<nkr_b200_msm_bases>();
     h->ctx = ctx;
-    NKR_TRY(msm_bases_build(h->bases, group, bases, false, n, true, 0, false, ctx->stream));
+    NKR_TRY(msm_bases_build_support(h->bases, group, bases, n, true, ctx->stream));
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
     NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[0]));
     NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[1]));
@@ -327,8 +327,8 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
                            float *device_ms)
 {
     NKR_REQUIRE(b && out, "null argument");
-    NKR_REQUIRE(n == b->bases.shape.n, "scalar count %llu does not match the %llu bases",
-                (unsigned long long)n, (unsigned long long)b->bases.shape.n);
+    NKR_REQUIRE(n == b->bases.n_full, "scalar count %llu does not match the %llu bases",
+                (unsigned long long)n, (unsigned long long)b->bases.n_full);
     NKR_TRY(ctx_check(b->ctx));
     cudaStream_t st = b->ctx->stream;
     cudaMemoryType mt = cudaMemoryTypeUnregistered;

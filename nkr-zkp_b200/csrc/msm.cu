@@ -4,6 +4,8 @@
 // product is compiled out of line (one body per kernel) to keep the hot loops
 // resident in the instruction cache.
 #define NKR_FIELD_MUL_OUTLINE 1
+#include <cstring>
+
 #include "msm.cuh"
 #include "scan.cuh"
 
@@ -50,15 +52,15 @@ __device__ __forceinline__ void for_each_digit(const Fr &s, int c, int W, Fn &&f
     }
 }
 
-__global__ void k_digits_count(const Fr *__restrict__ scalars, uint64_t n, int c, int W,
-                               bool folded, uint32_t B, Fr *__restrict__ canon,
-                               uint32_t *__restrict__ counts)
+__global__ void k_digits_count(const Fr *__restrict__ scalars, const uint32_t *__restrict__ gather,
+                               uint64_t n, int c, int W, bool folded, uint32_t B,
+                               Fr *__restrict__ canon, uint32_t *__restrict__ counts)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = i < n;
     Fr s = Fr::zero();
     if (live) {
-        s = from_mont(scalars[i]);
+        s = from_mont(scalars[gather ? gather[i] : i]);
         canon[i] = s;
     }
     const int lane = threadIdx.x & 31;
@@ -645,6 +647,40 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
     return NKR_B200_OK;
 }
 
+int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n, bool folded,
+                            cudaStream_t st)
+{
+    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
+    NKR_REQUIRE(n < (uint64_t(1) << 32), "support indices are 32-bit");
+    const size_t jac_sz = group == 1 ? 96 : 192;
+    const size_t z_off = jac_sz / 3 * 2, z_sz = jac_sz / 3;
+    const uint8_t *src = static_cast<const uint8_t *>(jac_host);
+    std::vector<uint32_t> idx;
+    idx.reserve(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint8_t *z = src + i * jac_sz + z_off;
+        bool zero = true;
+        for (size_t k = 0; k < z_sz && zero; k += 8) {
+            uint64_t w;
+            std::memcpy(&w, z + k, 8);
+            zero = w == 0;
+        }
+        if (!zero) idx.push_back(uint32_t(i));
+    }
+    if (idx.empty() && n) idx.push_back(0); // an all-infinity query still has one (zero) term
+    std::vector<uint8_t> packed(std::max<size_t>(idx.size(), 1) * jac_sz);
+    for (size_t j = 0; j < idx.size(); ++j)
+        std::memcpy(packed.data() + j * jac_sz, src + uint64_t(idx[j]) * jac_sz, jac_sz);
+    NKR_TRY(msm_bases_build(b, group, packed.data(), false, idx.size(), folded, 0, false, st));
+    b.n_full = n;
+    NKR_TRY(b.support.alloc(std::max<size_t>(idx.size(), 1) * 4, "msm support indices"));
+    if (!idx.empty())
+        NKR_CUDA(cudaMemcpyAsync(b.support.p, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    b.support_host = std::move(idx);
+    return NKR_B200_OK;
+}
+
 int msm_sort_alloc(MsmSort &s, const MsmShape &sh)
 {
     NKR_TRY(s.canon.alloc(std::max<uint64_t>(sh.n, 1) * sizeof(Fr), "msm canonical scalars"));
@@ -668,13 +704,14 @@ int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape)
     return NKR_B200_OK;
 }
 
-int msm_sort_run(const MsmShape &sh, MsmSort &s, const void *scalars_dev, cudaStream_t st)
+int msm_sort_run(const MsmShape &sh, MsmSort &s, const void *scalars_dev, cudaStream_t st,
+                 const uint32_t *gather)
 {
     const uint64_t n = sh.n;
     NKR_CUDA(cudaMemsetAsync(s.counts.p, 0, (sh.nb + 1) * 4, st));
     if (n) {
         k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>(
-            static_cast<const Fr *>(scalars_dev), n, sh.c, sh.W, sh.folded, sh.B, s.canon.as<Fr>(),
+            static_cast<const Fr *>(scalars_dev), gather, n, sh.c, sh.W, sh.folded, sh.B, s.canon.as<Fr>(),
             s.counts.as<uint32_t>());
         NKR_CHECK_LAUNCH();
     }
@@ -699,7 +736,7 @@ int msm_acc_run(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, c
 int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out_dev,
             cudaStream_t st)
 {
-    NKR_TRY(msm_sort_run(b.shape, s.sort, scalars_dev, st));
+    NKR_TRY(msm_sort_run(b.shape, s.sort, scalars_dev, st, b.gather()));
     return msm_acc_run(b, s.sort, s.acc, out_dev, st);
 }
 

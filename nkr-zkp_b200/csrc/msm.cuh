@@ -32,9 +32,16 @@
 //  5. output: Jacobian coordinates in the libff layout (X, Y, Z) with an
 //     arbitrary Z -- no device inversion on the critical path; the host
 //     normalises the few result points.
+//  6. support: the witness MSMs' bases are the proving key's queries, and a
+//     query point is the point at infinity for every variable absent from that
+//     matrix (about 2/3 of the B query in hash circuits).  Resident bases keep
+//     only the finite points and their indices; the sort gathers the scalars
+//     through those indices, so no entry, lane or bucket is spent on a point
+//     that adds nothing.
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 #include "curve.cuh"
@@ -94,7 +101,13 @@ struct MsmBases {
     int group = 1; // 1: G1, 2: G2
     MsmShape shape;
     DevBuf pts;
-    size_t device_bytes() const { return pts.bytes; }
+    // support form (msm_bases_build_support): pts holds only the finite points;
+    // support[i] is point i's index among the n_full original bases
+    DevBuf support;
+    std::vector<uint32_t> support_host;
+    uint64_t n_full = 0;
+    const uint32_t *gather() const { return support.p ? support.as<uint32_t>() : nullptr; }
+    size_t device_bytes() const { return pts.bytes + support.bytes; }
 };
 
 // Upload bases given in libff Jacobian layout (96 / 192 B per point) from host
@@ -103,6 +116,11 @@ struct MsmBases {
 // scalars held in bit-reversed order pair with their own bases.
 int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device, uint64_t n,
                     bool folded, int c_override, bool bitrev, cudaStream_t st);
+// Resident bases of the finite points among n host bases (libff Jacobian, Z = 0
+// is infinity); the scalars of this MSM are indexed by original point index
+// through gather().  Keeps one (infinite) point when all n are infinite.
+int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n, bool folded,
+                            cudaStream_t st);
 
 // Normalise n libff-layout Jacobian points (device) into affine (device).
 int jacobian_to_affine(int group, const void *jac, void *aff, uint64_t n, cudaStream_t st);
@@ -112,7 +130,9 @@ int msm_acc_alloc(MsmAcc &a, int group, const MsmShape &shape);
 int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape);
 
 // Sort the scalars Fr[n] (Montgomery, device) for the shape.
-int msm_sort_run(const MsmShape &shape, MsmSort &s, const void *scalars_dev, cudaStream_t st);
+// scalar i of the sort is scalars_dev[gather ? gather[i] : i]
+int msm_sort_run(const MsmShape &shape, MsmSort &s, const void *scalars_dev, cudaStream_t st,
+                 const uint32_t *gather = nullptr);
 // Accumulate / reduce with a finished sort of the same shape.  The result is
 // written to out_dev in libff Jacobian layout with an arbitrary Z (or Z = 0 for
 // infinity); normalise on the host (host/fr_host.hpp normalize_g1 / _g2).

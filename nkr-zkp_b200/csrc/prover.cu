@@ -13,6 +13,8 @@ namespace {
 
 constexpr size_t kOutBytes = 4 * 96 + 192; // ar, bs1, zk, qz (G1) + bs2 (G2)
 constexpr size_t kOutOffset[kNumMsm] = {0, 96, 192, 288, 384}; // A, B1, L, H, B2
+// issue order of the witness MSMs: the G2 MSM (longest) first
+constexpr int kWitnessOrder[4] = {kMsmB2, kMsmA, kMsmB1, kMsmL};
 
 // ---------------------------------------------------------------------------
 // blinding (protocol.cpp:85-94) with caller-supplied r, s
@@ -121,14 +123,18 @@ int prove_issue(nkr_b200_key *key, bool timed)
     NKR_CUDA(cudaEventRecord(key->ev_z, s0));
     if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[1], s0));
     // witness MSMs on their own streams, overlapping the H chain; one digit sort
-    // of z serves all four (same scalars, same window shape)
-    cudaStream_t sa = key->st[kMsmA];
-    NKR_CUDA(cudaStreamWaitEvent(sa, key->ev_z, 0));
-    NKR_TRY(msm_sort_run(key->bases[kMsmA].shape, key->sort_z, z, sa));
-    NKR_CUDA(cudaEventRecord(key->ev_sorted, sa));
-    for (int k : {kMsmB2, kMsmA, kMsmB1, kMsmL}) {
-        if (k != kMsmA) NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_sorted, 0));
-        NKR_TRY(msm_acc_run(key->bases[k], key->sort_z, key->acc[k], out + kOutOffset[k], key->st[k]));
+    // of z (gathered through the bases' support) per distinct support
+    for (int g = 0; g < key->n_sorts; ++g) {
+        const int o = key->sort_stream[g];
+        NKR_CUDA(cudaStreamWaitEvent(key->st[o], key->ev_z, 0));
+        NKR_TRY(msm_sort_run(key->bases[o].shape, key->sort_w[g], z, key->st[o],
+                             key->bases[o].gather()));
+        NKR_CUDA(cudaEventRecord(key->ev_sorted[g], key->st[o]));
+    }
+    for (int k : kWitnessOrder) {
+        const int g = key->sort_of[k];
+        if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_sorted[g], 0));
+        NKR_TRY(msm_acc_run(key->bases[k], key->sort_w[g], key->acc[k], out + kOutOffset[k], key->st[k]));
         NKR_CUDA(cudaEventRecord(key->ev_done[k], key->st[k]));
     }
     // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
@@ -189,11 +195,15 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
             return fail(NKR_B200_ECUDA);
         }
     }
-    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&key->ev_sorted, cudaEventDisableTiming) != cudaSuccess) {
+    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess) {
         set_error("event creation failed");
         return fail(NKR_B200_ECUDA);
     }
+    for (auto &e : key->ev_sorted)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            set_error("event creation failed");
+            return fail(NKR_B200_ECUDA);
+        }
     for (auto &e : key->ev_t)
         if (cudaEventCreate(&e) != cudaSuccess) {
             set_error("event creation failed");
@@ -205,17 +215,28 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
                             c->values[k], st));
     NKR_PREP(ntt_tables_build(key->ntt, logn, st));
     // proving key: normalise (hazard: CPU-setup keys are unnormalised Jacobian), fold windows
-    NKR_PREP(msm_bases_build(key->bases[kMsmA], 1, pk->a_query, false, c->cols, true, 0, false, st));
-    NKR_PREP(msm_bases_build(key->bases[kMsmB1], 1, pk->b_g1_query, false, c->cols, true, 0, false, st));
-    NKR_PREP(msm_bases_build(key->bases[kMsmL], 1, pk->l_query, false, c->cols, true, 0, false, st));
+    // witness queries keep only their finite points (variables present in the matrix)
+    NKR_PREP(msm_bases_build_support(key->bases[kMsmA], 1, pk->a_query, c->cols, true, st));
+    NKR_PREP(msm_bases_build_support(key->bases[kMsmB1], 1, pk->b_g1_query, c->cols, true, st));
+    NKR_PREP(msm_bases_build_support(key->bases[kMsmL], 1, pk->l_query, c->cols, true, st));
     NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, 0, true, st));
-    NKR_PREP(msm_bases_build(key->bases[kMsmB2], 2, pk->b_g2_query, false, c->cols, true, 0, false, st));
-    for (int k : {kMsmB1, kMsmL, kMsmB2})
-        if (!key->bases[k].shape.same_sort(key->bases[kMsmA].shape)) {
-            set_error("witness MSM shapes differ; the shared digit sort needs one shape");
-            return fail(NKR_B200_EINVAL);
+    NKR_PREP(msm_bases_build_support(key->bases[kMsmB2], 2, pk->b_g2_query, c->cols, true, st));
+    // MSMs with the same support (and so the same window shape) share a digit sort
+    key->n_sorts = 0;
+    for (int k : kWitnessOrder) {
+        int g = -1;
+        for (int h = 0; h < key->n_sorts && g < 0; ++h) {
+            const MsmBases &o = key->bases[key->sort_stream[h]];
+            if (o.shape.same_sort(key->bases[k].shape) && o.support_host == key->bases[k].support_host)
+                g = h;
         }
-    NKR_PREP(msm_sort_alloc(key->sort_z, key->bases[kMsmA].shape));
+        if (g < 0) {
+            g = key->n_sorts++;
+            key->sort_stream[g] = k;
+            NKR_PREP(msm_sort_alloc(key->sort_w[g], key->bases[k].shape));
+        }
+        key->sort_of[k] = g;
+    }
     NKR_PREP(msm_sort_alloc(key->sort_h, key->bases[kMsmH].shape));
     for (int k = 0; k < kNumMsm; ++k)
         NKR_PREP(msm_acc_alloc(key->acc[k], key->bases[k].group, key->bases[k].shape));
@@ -420,7 +441,8 @@ void nkr_b200_key_free(nkr_b200_key *key)
         if (key->ev_done[k]) cudaEventDestroy(key->ev_done[k]);
     }
     if (key->ev_z) cudaEventDestroy(key->ev_z);
-    if (key->ev_sorted) cudaEventDestroy(key->ev_sorted);
+    for (auto e : key->ev_sorted)
+        if (e) cudaEventDestroy(e);
     for (auto e : key->ev_t)
         if (e) cudaEventDestroy(e);
     if (key->pinned_out) cudaFreeHost(key->pinned_out);
@@ -437,6 +459,7 @@ uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
     for (int k = 0; k < 3; ++k)
         b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].values.bytes;
     for (int k = 0; k < nkr::kNumMsm; ++k) b += key->bases[k].device_bytes() + key->acc[k].device_bytes();
-    b += key->sort_z.device_bytes() + key->sort_h.device_bytes();
+    for (int g = 0; g < key->n_sorts; ++g) b += key->sort_w[g].device_bytes();
+    b += key->sort_h.device_bytes();
     return b;
 }

@@ -36,7 +36,12 @@ struct nkr_b200_key {
     nkr::CsrDevice mat[3];
     nkr::NttTables ntt;
     nkr::MsmBases bases[nkr::kNumMsm];
-    nkr::MsmSort sort_z;               // digit sort of the witness, shared by the 4 witness MSMs
+    // digit sorts of the witness: one per distinct support among the 4 witness MSMs
+    // (B1 and B2 always share one); sort g runs on the stream of MSM sort_stream[g]
+    nkr::MsmSort sort_w[4];
+    int n_sorts = 0;
+    int sort_of[nkr::kNumMsm] = {};
+    int sort_stream[4] = {};
     nkr::MsmSort sort_h;               // digit sort of H
     nkr::MsmAcc acc[nkr::kNumMsm];
     nkr::DevBuf z, az, bz, cz, h;
@@ -44,7 +49,7 @@ struct nkr_b200_key {
     nkr::DevBuf pk_const; // alpha_g1, beta_g1, delta_g1 (G1 affine) and beta_g2, delta_g2 (G2 affine)
     nkr::DevBuf blind_io; // r, s in; proof out
     cudaStream_t st[nkr::kNumMsm] = {};
-    cudaEvent_t ev_z = nullptr, ev_sorted = nullptr, ev_done[nkr::kNumMsm] = {};
+    cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[nkr::kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
     void *pinned_in = nullptr;  // witness staging (cols * 32 B)
     void *pinned_out = nullptr; // results staging (576 B + proof)

@@ -69,6 +69,23 @@ def test_msm_edge_cases(ctx, orc, rng, group, folded):
     _check(ctx, orc, group, aff, sc, folded)
 
 
+@pytest.mark.parametrize("group", [1, 2])
+def test_msm_mostly_and_all_infinity_bases(ctx, orc, rng, group):
+    """Resident bases keep only their finite points (a B query is ~70% infinity)
+    and gather the scalars through the kept indices; all-infinity bases give 0."""
+    n = 2000
+    aff = _points(orc, group, n, rng, distinct=200)
+    w = 4 * group
+    inf = np.nonzero(rng.random(n) < 0.7)[0]
+    aff[inf] = 0
+    aff[inf, w:w + 4] = O.fq_mont(1)
+    sc = O.random_fr(n, rng)
+    _check(ctx, orc, group, aff, sc, folded=True)
+    aff[:] = 0
+    aff[:, w:w + 4] = O.fq_mont(1)
+    _check(ctx, orc, group, aff, sc, folded=True)
+
+
 @pytest.mark.parametrize("folded", [False, True])
 def test_msm_all_zero_scalars_is_infinity(ctx, orc, rng, folded):
     aff = _points(orc, 1, 50, rng)
