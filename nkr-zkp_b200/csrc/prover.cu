@@ -1,6 +1,7 @@
 // Groth16 prepare / prove / blind on one B200 (design notes in prover.cuh).
 // The blinding kernel chains scalar multiplications: out-of-line products.
 #define NKR_FIELD_MUL_OUTLINE 1
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -11,7 +12,6 @@ namespace nkr {
 
 namespace {
 
-constexpr size_t kOutBytes = 4 * 96 + 192; // ar, bs1, zk, qz (G1) + bs2 (G2)
 constexpr size_t kOutOffset[kNumMsm] = {0, 96, 192, 288, 384}; // A, B1, L, H, B2
 // issue order of the witness MSMs: the G2 MSM (longest) first
 constexpr int kWitnessOrder[4] = {kMsmB2, kMsmA, kMsmB1, kMsmL};
@@ -92,50 +92,130 @@ void normalize_raw(void *raw576)
     host::normalize_g2(o + 384);
 }
 
+void raw_from_bytes(const void *raw576, nkr_b200_raw_proof *res)
+{
+    const uint8_t *o = static_cast<const uint8_t *>(raw576);
+    std::memcpy(res->ar, o + 0, 96);
+    std::memcpy(res->bs1, o + 96, 96);
+    std::memcpy(res->zk, o + 192, 96);
+    std::memcpy(res->qz, o + 288, 96);
+    std::memcpy(res->bs2, o + 384, 192);
+}
+
 namespace {
 
-int check_witness_ptr(const void *p, cudaMemoryType *type)
+cudaMemcpyKind copy_kind_from(const void *p)
 {
     cudaPointerAttributes attr{};
-    cudaError_t e = cudaPointerGetAttributes(&attr, p);
-    if (e != cudaSuccess) {
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
         cudaGetLastError();
-        *type = cudaMemoryTypeUnregistered;
-        return NKR_B200_OK;
+        return cudaMemcpyHostToDevice;
     }
-    *type = attr.type;
-    return NKR_B200_OK;
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged
+               ? cudaMemcpyDeviceToDevice
+               : cudaMemcpyHostToDevice;
+}
+
+bool is_pageable(const void *p)
+{
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return attr.type == cudaMemoryTypeUnregistered;
 }
 
 } // namespace
 
-int prove_issue(nkr_b200_key *key, bool timed)
+ProveSlot::~ProveSlot()
 {
-    cudaStream_t s0 = key->st[kMsmH];
+    for (auto s : st)
+        if (s) cudaStreamSynchronize(s);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (int k = 0; k < kNumMsm; ++k) {
+        if (st[k]) cudaStreamDestroy(st[k]);
+        if (ev_done[k]) cudaEventDestroy(ev_done[k]);
+    }
+    for (cudaEvent_t e : {ev_z, ev_wit[0], ev_wit[1]})
+        if (e) cudaEventDestroy(e);
+    for (auto e : ev_sorted)
+        if (e) cudaEventDestroy(e);
+    for (auto e : ev_t)
+        if (e) cudaEventDestroy(e);
+    for (auto p : pinned_wit)
+        if (p) cudaFreeHost(p);
+    if (pinned_out) cudaFreeHost(pinned_out);
+}
+
+int slot_add(nkr_b200_key *key)
+{
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    auto slot = std::make_unique<ProveSlot>();
+    ProveSlot *sl = slot.get();
+    for (int k = 0; k < kNumMsm; ++k) {
+        NKR_CUDA(cudaStreamCreateWithFlags(&sl->st[k], cudaStreamNonBlocking));
+        NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_done[k], cudaEventDisableTiming));
+    }
+    NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_z, cudaEventDisableTiming));
+    for (auto &e : sl->ev_sorted) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : sl->ev_wit) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : sl->ev_t) NKR_CUDA(cudaEventCreate(&e));
+    size_t bytes = 0;
+    for (int g = 0; g < key->n_sorts; ++g) {
+        NKR_TRY(msm_sort_alloc(sl->sort_w[g], key->bases[key->sort_stream[g]].shape));
+        bytes += sl->sort_w[g].device_bytes();
+    }
+    NKR_TRY(msm_sort_alloc(sl->sort_h, key->bases[kMsmH].shape));
+    bytes += sl->sort_h.device_bytes();
+    for (int k = 0; k < kNumMsm; ++k) {
+        NKR_TRY(msm_acc_alloc(sl->acc[k], key->bases[k].group, key->bases[k].shape));
+        bytes += sl->acc[k].device_bytes();
+    }
+    NKR_TRY(sl->z.alloc(key->cols * 32, "witness"));
+    NKR_TRY(sl->az.alloc(key->rows * 32, "az"));
+    NKR_TRY(sl->bz.alloc(key->rows * 32, "bz"));
+    NKR_TRY(sl->cz.alloc(key->rows * 32, "cz"));
+    NKR_TRY(sl->h.alloc(key->rows * 32, "H"));
+    NKR_TRY(sl->out.alloc(kOutBytes, "proof points"));
+    bytes += sl->z.bytes + 4 * sl->az.bytes + sl->out.bytes;
+    if (cudaHostAlloc(&sl->pinned_out, kOutBytes + 384, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("pinned host allocation failed");
+        return NKR_B200_ENOMEM;
+    }
+    key->slot_bytes = bytes;
+    key->slots.push_back(std::move(slot));
+    return NKR_B200_OK;
+}
+
+int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed)
+{
+    cudaStream_t s0 = sl->main();
     const uint64_t rows = key->rows;
-    Fr *z = key->z.as<Fr>();
-    Fr *az = key->az.as<Fr>(), *bz = key->bz.as<Fr>(), *cz = key->cz.as<Fr>(), *h = key->h.as<Fr>();
-    uint8_t *out = key->out.as<uint8_t>();
-    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[0], s0));
+    Fr *z = sl->z.as<Fr>();
+    Fr *az = sl->az.as<Fr>(), *bz = sl->bz.as<Fr>(), *cz = sl->cz.as<Fr>(), *h = sl->h.as<Fr>();
+    uint8_t *out = sl->out.as<uint8_t>();
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[0], s0));
     const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
     Fr *ys[3] = {az, bz, cz};
     NKR_TRY(spmv_multi(mats, 3, z, ys, s0));
-    NKR_CUDA(cudaEventRecord(key->ev_z, s0));
-    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[1], s0));
+    NKR_CUDA(cudaEventRecord(sl->ev_z, s0));
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[1], s0));
     // witness MSMs on their own streams, overlapping the H chain; one digit sort
     // of z (gathered through the bases' support) per distinct support
     for (int g = 0; g < key->n_sorts; ++g) {
         const int o = key->sort_stream[g];
-        NKR_CUDA(cudaStreamWaitEvent(key->st[o], key->ev_z, 0));
-        NKR_TRY(msm_sort_run(key->bases[o].shape, key->sort_w[g], z, key->st[o],
-                             key->bases[o].gather()));
-        NKR_CUDA(cudaEventRecord(key->ev_sorted[g], key->st[o]));
+        NKR_CUDA(cudaStreamWaitEvent(sl->st[o], sl->ev_z, 0));
+        NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], z, sl->st[o], key->bases[o].gather()));
+        NKR_CUDA(cudaEventRecord(sl->ev_sorted[g], sl->st[o]));
     }
     for (int k : kWitnessOrder) {
         const int g = key->sort_of[k];
-        if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(key->st[k], key->ev_sorted[g], 0));
-        NKR_TRY(msm_acc_run(key->bases[k], key->sort_w[g], key->acc[k], out + kOutOffset[k], key->st[k]));
-        NKR_CUDA(cudaEventRecord(key->ev_done[k], key->st[k]));
+        if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(sl->st[k], sl->ev_sorted[g], 0));
+        NKR_TRY(msm_acc_run(key->bases[k], sl->sort_w[g], sl->acc[k], out + kOutOffset[k], sl->st[k]));
+        NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
     }
     // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
     const NttTables &T = key->ntt;
@@ -146,13 +226,85 @@ int prove_issue(nkr_b200_key *key, bool timed)
     }
     NKR_TRY(fr_quotient_pointwise(az, bz, cz, h, rows, cst + kConstZinv, s0));
     NKR_TRY(ntt_dif(T, h, true, nullptr, T.t2.as<Fr>(), nullptr, s0));
-    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[2], s0));
-    NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, key->sort_h, h, s0));
-    NKR_TRY(msm_acc_run(key->bases[kMsmH], key->sort_h, key->acc[kMsmH], out + kOutOffset[kMsmH], s0));
-    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[3], s0));
-    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2})
-        NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
-    if (timed) NKR_CUDA(cudaEventRecord(key->ev_t[4], s0));
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[2], s0));
+    NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, sl->sort_h, h, s0));
+    NKR_TRY(msm_acc_run(key->bases[kMsmH], sl->sort_h, sl->acc[kMsmH], out + kOutOffset[kMsmH], s0));
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[3], s0));
+    for (int k : kWitnessOrder) NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_done[k], 0));
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[4], s0));
+    return NKR_B200_OK;
+}
+
+int slot_capture(nkr_b200_key *key, ProveSlot *sl)
+{
+    if (sl->graph_exec) return NKR_B200_OK;
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    for (auto s : sl->st) NKR_CUDA(cudaStreamSynchronize(s));
+    cudaStream_t s0 = sl->main();
+    const unsigned long long before = g_kernel_launches.load();
+    NKR_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
+    const int s = prove_issue(key, sl, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s0, &g);
+    // capturing records kernels, it launches none
+    g_kernel_launches.fetch_sub(g_kernel_launches.load() - before);
+    if (s != NKR_B200_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (s == NKR_B200_OK) set_error("prove graph capture failed: %s", cudaGetErrorString(e));
+        return s != NKR_B200_OK ? s : NKR_B200_ECUDA;
+    }
+    size_t nn = 0;
+    NKR_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    NKR_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    unsigned long long kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        NKR_CUDA(cudaGraphNodeGetType(nd, &t));
+        kernels += t == cudaGraphNodeTypeKernel;
+    }
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        set_error("prove graph instantiation failed: %s", cudaGetErrorString(ei));
+        return NKR_B200_ECUDA;
+    }
+    sl->graph = g;
+    sl->graph_exec = ex;
+    sl->graph_kernels = kernels;
+    return NKR_B200_OK;
+}
+
+int slot_upload_witness(nkr_b200_key *key, ProveSlot *sl, const void *witness)
+{
+    const size_t bytes = key->cols * 32;
+    cudaStream_t s0 = sl->main();
+    if (!is_pageable(witness)) {
+        NKR_CUDA(cudaMemcpyAsync(sl->z.p, witness, bytes, copy_kind_from(witness), s0));
+        return NKR_B200_OK;
+    }
+    // pageable: stage through the slot's pinned double buffer so the copy is asynchronous
+    const int b = sl->wit_next;
+    sl->wit_next ^= 1;
+    if (!sl->pinned_wit[b] && cudaHostAlloc(&sl->pinned_wit[b], bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        sl->pinned_wit[b] = nullptr;
+        set_error("pinned witness staging allocation failed");
+        return NKR_B200_ENOMEM;
+    }
+    NKR_CUDA(cudaEventSynchronize(sl->ev_wit[b]));
+    std::memcpy(sl->pinned_wit[b], witness, bytes);
+    NKR_CUDA(cudaMemcpyAsync(sl->z.p, sl->pinned_wit[b], bytes, cudaMemcpyHostToDevice, s0));
+    NKR_CUDA(cudaEventRecord(sl->ev_wit[b], s0));
+    return NKR_B200_OK;
+}
+
+int slot_launch(ProveSlot *sl)
+{
+    NKR_CUDA(cudaGraphLaunch(sl->graph_exec, sl->main()));
+    g_kernel_launches.fetch_add(sl->graph_kernels, std::memory_order_relaxed);
     return NKR_B200_OK;
 }
 
@@ -188,34 +340,13 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
         s = (expr);                                                                             \
         if (s != NKR_B200_OK) return fail(s);                                                   \
     } while (0)
-    for (int k = 0; k < kNumMsm; ++k) {
-        if (cudaStreamCreateWithFlags(&key->st[k], cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&key->ev_done[k], cudaEventDisableTiming) != cudaSuccess) {
-            set_error("stream/event creation failed");
-            return fail(NKR_B200_ECUDA);
-        }
-    }
-    if (cudaEventCreateWithFlags(&key->ev_z, cudaEventDisableTiming) != cudaSuccess) {
-        set_error("event creation failed");
-        return fail(NKR_B200_ECUDA);
-    }
-    for (auto &e : key->ev_sorted)
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
-            set_error("event creation failed");
-            return fail(NKR_B200_ECUDA);
-        }
-    for (auto &e : key->ev_t)
-        if (cudaEventCreate(&e) != cudaSuccess) {
-            set_error("event creation failed");
-            return fail(NKR_B200_ECUDA);
-        }
-    cudaStream_t st = key->st[kMsmH];
+    cudaStream_t st = ctx->stream;
     for (int k = 0; k < 3; ++k)
         NKR_PREP(csr_upload(key->mat[k], c->rows, c->cols, c->row_ptr[k], c->col_idx[k],
                             c->values[k], st));
     NKR_PREP(ntt_tables_build(key->ntt, logn, st));
-    // proving key: normalise (hazard: CPU-setup keys are unnormalised Jacobian), fold windows
-    // witness queries keep only their finite points (variables present in the matrix)
+    // proving key: normalise (hazard: CPU-setup keys are unnormalised Jacobian), fold
+    // windows; witness queries keep only their finite points (variables present in the matrix)
     NKR_PREP(msm_bases_build_support(key->bases[kMsmA], 1, pk->a_query, c->cols, true, st));
     NKR_PREP(msm_bases_build_support(key->bases[kMsmB1], 1, pk->b_g1_query, c->cols, true, st));
     NKR_PREP(msm_bases_build_support(key->bases[kMsmL], 1, pk->l_query, c->cols, true, st));
@@ -233,19 +364,9 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
         if (g < 0) {
             g = key->n_sorts++;
             key->sort_stream[g] = k;
-            NKR_PREP(msm_sort_alloc(key->sort_w[g], key->bases[k].shape));
         }
         key->sort_of[k] = g;
     }
-    NKR_PREP(msm_sort_alloc(key->sort_h, key->bases[kMsmH].shape));
-    for (int k = 0; k < kNumMsm; ++k)
-        NKR_PREP(msm_acc_alloc(key->acc[k], key->bases[k].group, key->bases[k].shape));
-    NKR_PREP(key->z.alloc(c->cols * 32, "witness"));
-    NKR_PREP(key->az.alloc(c->rows * 32, "az"));
-    NKR_PREP(key->bz.alloc(c->rows * 32, "bz"));
-    NKR_PREP(key->cz.alloc(c->rows * 32, "cz"));
-    NKR_PREP(key->h.alloc(c->rows * 32, "H"));
-    NKR_PREP(key->out.alloc(kOutBytes, "proof points"));
     NKR_PREP(key->blind_io.alloc(64 + 384, "blinding io"));
     // PK constants: libff Jacobian -> affine
     {
@@ -270,10 +391,7 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
             return fail(NKR_B200_ECUDA);
         }
     }
-    if (cudaHostAlloc(&key->pinned_out, kOutBytes + 384, cudaHostAllocDefault) != cudaSuccess) {
-        set_error("pinned host allocation failed");
-        return fail(NKR_B200_ENOMEM);
-    }
+    NKR_PREP(slot_add(key));
 #undef NKR_PREP
     *out = key;
     return NKR_B200_OK;
@@ -285,31 +403,21 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     NKR_REQUIRE(n == key->cols, "witness has %llu elements, the circuit has %llu columns",
                 (unsigned long long)n, (unsigned long long)key->cols);
     NKR_CUDA(cudaSetDevice(key->ctx->device));
-    cudaStream_t s0 = key->st[kMsmH];
-    // the previous prove's witness MSMs must be done before z is overwritten
-    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
-    cudaMemoryType mt;
-    check_witness_ptr(witness, &mt);
-    NKR_CUDA(cudaMemcpyAsync(key->z.p, witness, n * 32,
-                             mt == cudaMemoryTypeDevice ? cudaMemcpyDeviceToDevice
-                                                        : cudaMemcpyHostToDevice,
-                             s0));
-    NKR_TRY(prove_issue(key, true));
-    NKR_CUDA(cudaMemcpyAsync(key->pinned_out, key->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
+    ProveSlot *sl = key->slots[0].get();
+    cudaStream_t s0 = sl->main();
+    // s0 is ordered after the previous prove's joins, so z is free to overwrite
+    NKR_CUDA(cudaMemcpyAsync(sl->z.p, witness, n * 32, copy_kind_from(witness), s0));
+    NKR_TRY(prove_issue(key, sl, true));
+    NKR_CUDA(cudaMemcpyAsync(sl->pinned_out, sl->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
     NKR_CUDA(cudaStreamSynchronize(s0));
-    normalize_raw(key->pinned_out);
-    const uint8_t *o = static_cast<const uint8_t *>(key->pinned_out);
-    std::memcpy(res->ar, o + 0, 96);
-    std::memcpy(res->bs1, o + 96, 96);
-    std::memcpy(res->zk, o + 192, 96);
-    std::memcpy(res->qz, o + 288, 96);
-    std::memcpy(res->bs2, o + 384, 192);
+    normalize_raw(sl->pinned_out);
+    raw_from_bytes(sl->pinned_out, res);
     float ms[4];
-    for (int i = 0; i < 4; ++i) NKR_CUDA(cudaEventElapsedTime(&ms[i], key->ev_t[i], key->ev_t[i + 1]));
+    for (int i = 0; i < 4; ++i) NKR_CUDA(cudaEventElapsedTime(&ms[i], sl->ev_t[i], sl->ev_t[i + 1]));
     key->times.spmv_ms = ms[0];
     key->times.quotient_ms = ms[1];
     key->times.quotient_msm_ms = ms[2];
-    NKR_CUDA(cudaEventElapsedTime(&key->times.total_ms, key->ev_t[0], key->ev_t[4]));
+    NKR_CUDA(cudaEventElapsedTime(&key->times.total_ms, sl->ev_t[0], sl->ev_t[4]));
     key->times.witness_msms_ms = key->times.total_ms - ms[0];
     key->have_times = true;
     return NKR_B200_OK;
@@ -320,10 +428,11 @@ int key_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r, c
 {
     NKR_REQUIRE(key && raw && r && s && res, "null argument");
     NKR_CUDA(cudaSetDevice(key->ctx->device));
-    cudaStream_t s0 = key->st[kMsmH];
-    uint8_t *host = static_cast<uint8_t *>(key->pinned_out) + kOutBytes; // 384 B staging
+    ProveSlot *sl = key->slots[0].get();
+    cudaStream_t s0 = sl->main();
+    uint8_t *host = static_cast<uint8_t *>(sl->pinned_out) + kOutBytes; // 384 B staging
     uint8_t *dev = key->blind_io.as<uint8_t>();
-    // raw points go to key->out (device) in libff layout; r, s to blind_io[0, 64)
+    // raw points go to the slot's out (device) in libff layout; r, s to blind_io[0, 64)
     uint8_t staging[kOutBytes];
     std::memcpy(staging + 0, raw->ar, 96);
     std::memcpy(staging + 96, raw->bs1, 96);
@@ -331,11 +440,11 @@ int key_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r, c
     std::memcpy(staging + 288, raw->qz, 96);
     std::memcpy(staging + 384, raw->bs2, 192);
     NKR_CUDA(cudaStreamSynchronize(s0));
-    NKR_CUDA(cudaMemcpy(key->out.p, staging, kOutBytes, cudaMemcpyHostToDevice));
+    NKR_CUDA(cudaMemcpy(sl->out.p, staging, kOutBytes, cudaMemcpyHostToDevice));
     NKR_CUDA(cudaMemcpy(dev, r, 32, cudaMemcpyHostToDevice));
     NKR_CUDA(cudaMemcpy(dev + 32, s, 32, cudaMemcpyHostToDevice));
-    k_blind<<<1, 7 * 32, 0, s0>>>(key->pk_const.as<uint8_t>(), key->out.as<uint8_t>(),
-                              reinterpret_cast<const Fr *>(dev), dev + 64);
+    k_blind<<<1, 7 * 32, 0, s0>>>(key->pk_const.as<uint8_t>(), sl->out.as<uint8_t>(),
+                                  reinterpret_cast<const Fr *>(dev), dev + 64);
     NKR_CHECK_LAUNCH();
     NKR_CUDA(cudaMemcpyAsync(host, dev + 64, 384, cudaMemcpyDeviceToHost, s0));
     NKR_CUDA(cudaStreamSynchronize(s0));
@@ -349,8 +458,8 @@ int key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
 {
     NKR_REQUIRE(key, "null key");
     NKR_CUDA(cudaSetDevice(key->ctx->device));
-    cudaStream_t s0 = key->st[kMsmH];
-    for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) NKR_CUDA(cudaStreamWaitEvent(s0, key->ev_done[k], 0));
+    ProveSlot *sl = key->slots[0].get();
+    cudaStream_t s0 = sl->main();
     const uint64_t rows = key->rows;
     DevBuf tmp;
     NKR_TRY(tmp.alloc(4 * rows * 32, "intermediate scratch"));
@@ -358,9 +467,9 @@ int key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
     // the SpMV is a pure function of the resident witness: recompute az, bz, cz
     const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
     Fr *ys[3] = {t, t + rows, t + 2 * rows};
-    NKR_TRY(spmv_multi(mats, 3, key->z.as<Fr>(), ys, s0));
+    NKR_TRY(spmv_multi(mats, 3, sl->z.as<Fr>(), ys, s0));
     // H is held in bit-reversed order; return it in natural order
-    NKR_TRY(ntt_bitrev_permute(key->h.as<Fr>(), t + 3 * rows, rows, nullptr, nullptr, s0));
+    NKR_TRY(ntt_bitrev_permute(sl->h.as<Fr>(), t + 3 * rows, rows, nullptr, nullptr, s0));
     void *dst[4] = {az, bz, cz, h};
     for (int i = 0; i < 4; ++i)
         if (dst[i]) NKR_CUDA(cudaMemcpyAsync(dst[i], t + i * rows, rows * 32, cudaMemcpyDeviceToHost, s0));
@@ -368,63 +477,91 @@ int key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
     return NKR_B200_OK;
 }
 
+namespace {
+
+constexpr int kMaxSlotsPerKey = 4;
+constexpr size_t kSlotHeadroom = size_t(1) << 30; // free HBM kept after admitting a slot
+
+// Grows the key's slots toward `want` while free HBM admits another one.
+int admit_slots(nkr_b200_key *key, int want)
+{
+    NKR_CUDA(cudaSetDevice(key->ctx->device));
+    while (int(key->slots.size()) < want) {
+        size_t free_b = 0, total_b = 0;
+        NKR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if (free_b < key->slot_bytes + kSlotHeadroom) break;
+        NKR_TRY(slot_add(key));
+    }
+    return NKR_B200_OK;
+}
+
+} // namespace
+
 int key_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
                     nkr_b200_raw_proof *out)
 {
     NKR_REQUIRE(keys && witnesses && out && count >= 0, "null argument");
-    std::vector<std::vector<uint8_t>> staged(count);
-    // issue every proof without host synchronisation; proofs on different keys overlap
-    std::vector<void *> pinned(count, nullptr);
+    std::vector<nkr_b200_key *> distinct;
+    std::vector<int> per_key;
+    for (int i = 0; i < count; ++i) {
+        NKR_REQUIRE(keys[i] && witnesses[i], "null key or witness at %d", i);
+        size_t j = 0;
+        while (j < distinct.size() && distinct[j] != keys[i]) ++j;
+        if (j == distinct.size()) {
+            distinct.push_back(keys[i]);
+            per_key.push_back(0);
+        }
+        ++per_key[j];
+    }
+    // slots: up to kMaxSlotsPerKey proofs of one key in flight, admitted by free HBM;
+    // each slot replays its captured prove graph
+    for (size_t j = 0; j < distinct.size(); ++j) {
+        NKR_TRY(admit_slots(distinct[j], std::min(per_key[j], kMaxSlotsPerKey)));
+        for (auto &sl : distinct[j]->slots) NKR_TRY(slot_capture(distinct[j], sl.get()));
+    }
+    void *res = nullptr;
+    if (count) {
+        NKR_CUDA(cudaSetDevice(keys[0]->ctx->device));
+        if (cudaHostAlloc(&res, size_t(count) * kOutBytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("pinned result allocation failed");
+            return NKR_B200_ENOMEM;
+        }
+    }
+    std::vector<size_t> next(distinct.size(), 0);
+    std::vector<ProveSlot *> used;
     int status = NKR_B200_OK;
     for (int i = 0; i < count && status == NKR_B200_OK; ++i) {
         nkr_b200_key *key = keys[i];
-        if (!key) {
-            set_error("null key at %d", i);
-            status = NKR_B200_EINVAL;
-            break;
-        }
-        cudaSetDevice(key->ctx->device);
-        cudaStream_t s0 = key->st[kMsmH];
-        for (int k : {kMsmA, kMsmB1, kMsmL, kMsmB2}) cudaStreamWaitEvent(s0, key->ev_done[k], 0);
-        cudaMemoryType mt;
-        check_witness_ptr(witnesses[i], &mt);
-        if (cudaMemcpyAsync(key->z.p, witnesses[i], key->cols * 32,
-                            mt == cudaMemoryTypeDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                            s0) != cudaSuccess) {
-            set_error("witness upload failed");
+        const size_t j = size_t(std::find(distinct.begin(), distinct.end(), key) - distinct.begin());
+        ProveSlot *sl = key->slots[next[j]++ % key->slots.size()].get();
+        if (cudaSetDevice(key->ctx->device) != cudaSuccess) {
+            set_error("cudaSetDevice failed");
             status = NKR_B200_ECUDA;
             break;
         }
-        status = prove_issue(key, false);
-        if (status != NKR_B200_OK) break;
-        if (cudaHostAlloc(&pinned[i], kOutBytes, cudaHostAllocDefault) != cudaSuccess) {
-            set_error("pinned allocation failed");
-            status = NKR_B200_ENOMEM;
-            break;
-        }
-        cudaMemcpyAsync(pinned[i], key->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0);
-    }
-    for (int i = 0; i < count; ++i) {
-        if (!pinned[i]) continue;
-        cudaStreamSynchronize(keys[i]->st[kMsmH]);
-        if (status == NKR_B200_OK) {
-            normalize_raw(pinned[i]);
-            const uint8_t *o = static_cast<const uint8_t *>(pinned[i]);
-            std::memcpy(out[i].ar, o, 96);
-            std::memcpy(out[i].bs1, o + 96, 96);
-            std::memcpy(out[i].zk, o + 192, 96);
-            std::memcpy(out[i].qz, o + 288, 96);
-            std::memcpy(out[i].bs2, o + 384, 192);
-        }
-        cudaFreeHost(pinned[i]);
-    }
-    if (status == NKR_B200_OK) {
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            set_error("batch: %s", cudaGetErrorString(e));
+        status = slot_upload_witness(key, sl, witnesses[i]);
+        if (status == NKR_B200_OK) status = slot_launch(sl);
+        if (status == NKR_B200_OK &&
+            cudaMemcpyAsync(static_cast<uint8_t *>(res) + size_t(i) * kOutBytes, sl->out.p, kOutBytes,
+                            cudaMemcpyDeviceToHost, sl->main()) != cudaSuccess) {
+            set_error("result download failed");
             status = NKR_B200_ECUDA;
         }
+        if (std::find(used.begin(), used.end(), sl) == used.end()) used.push_back(sl);
     }
+    for (ProveSlot *sl : used)
+        if (cudaStreamSynchronize(sl->main()) != cudaSuccess && status == NKR_B200_OK) {
+            set_error("batch: %s", cudaGetErrorString(cudaGetLastError()));
+            status = NKR_B200_ECUDA;
+        }
+    if (status == NKR_B200_OK)
+        for (int i = 0; i < count; ++i) {
+            uint8_t *o = static_cast<uint8_t *>(res) + size_t(i) * kOutBytes;
+            normalize_raw(o);
+            raw_from_bytes(o, &out[i]);
+        }
+    if (res) cudaFreeHost(res);
     return status;
 }
 
@@ -434,32 +571,17 @@ void nkr_b200_key_free(nkr_b200_key *key)
 {
     if (!key) return;
     if (key->ctx) cudaSetDevice(key->ctx->device);
-    for (int k = 0; k < nkr::kNumMsm; ++k)
-        if (key->st[k]) cudaStreamSynchronize(key->st[k]);
-    for (int k = 0; k < nkr::kNumMsm; ++k) {
-        if (key->st[k]) cudaStreamDestroy(key->st[k]);
-        if (key->ev_done[k]) cudaEventDestroy(key->ev_done[k]);
-    }
-    if (key->ev_z) cudaEventDestroy(key->ev_z);
-    for (auto e : key->ev_sorted)
-        if (e) cudaEventDestroy(e);
-    for (auto e : key->ev_t)
-        if (e) cudaEventDestroy(e);
-    if (key->pinned_out) cudaFreeHost(key->pinned_out);
-    if (key->pinned_in) cudaFreeHost(key->pinned_in);
+    key->slots.clear();
     delete key;
 }
 
 uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
 {
     if (!key) return 0;
-    uint64_t b = key->ntt.device_bytes() + key->z.bytes + key->az.bytes + key->bz.bytes +
-                 key->cz.bytes + key->h.bytes + key->out.bytes + key->pk_const.bytes +
-                 key->blind_io.bytes;
+    uint64_t b = key->ntt.device_bytes() + key->pk_const.bytes + key->blind_io.bytes;
     for (int k = 0; k < 3; ++k)
         b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].values.bytes;
-    for (int k = 0; k < nkr::kNumMsm; ++k) b += key->bases[k].device_bytes() + key->acc[k].device_bytes();
-    for (int g = 0; g < key->n_sorts; ++g) b += key->sort_w[g].device_bytes();
-    b += key->sort_h.device_bytes();
+    for (int k = 0; k < nkr::kNumMsm; ++k) b += key->bases[k].device_bytes();
+    b += key->slot_bytes * key->slots.size();
     return b;
 }

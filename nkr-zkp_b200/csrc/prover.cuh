@@ -3,13 +3,22 @@
 // (protocols/groth16/backends/cuda/src/groth16_backend.cu:214-279) and the CPU
 // backend's prove (backends/cpu/src/backend.cpp:156-201).
 //
-// Streams: after the witness upload and the SpMV, the four witness MSMs
-// (a, b_g1, l on G1 and b_g2 on G2) run on their own streams while the main
-// stream computes H (7 transforms) and then the H MSM; the reference runs every
-// stage serially with a device sync after each.
+// A key holds what every proof of the circuit reads (CSR matrices, NTT tables,
+// folded MSM bases) once.  Everything one proof writes lives in a prove slot:
+// witness and quotient vectors, digit sorts, bucket scratch, result points,
+// five streams and their events, and a CUDA graph of the whole prove.  Slot 0
+// serves nkr_b200_prove; batches and the request server add slots so several
+// proofs of one key are in flight at once.
+//
+// Streams of a slot: after the witness upload and the SpMV, the four witness
+// MSMs (a, b_g1, l on G1 and b_g2 on G2) run on their own streams while the
+// main stream computes H (7 transforms) and then the H MSM; the reference runs
+// every stage serially with a device sync after each.
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <vector>
 
 #include "common.cuh"
 #include "field.cuh"
@@ -26,6 +35,29 @@ struct nkr_b200_ctx {
 namespace nkr {
 
 enum { kMsmA = 0, kMsmB1 = 1, kMsmL = 2, kMsmH = 3, kMsmB2 = 4, kNumMsm = 5 };
+constexpr size_t kOutBytes = 4 * 96 + 192; // ar, bs1, zk, qz (G1) + bs2 (G2), libff layout
+
+struct ProveSlot {
+    MsmSort sort_w[4]; // witness digit sorts, one per distinct support
+    MsmSort sort_h;    // digit sort of H
+    MsmAcc acc[kNumMsm];
+    DevBuf z, az, bz, cz, h;
+    DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
+    cudaStream_t st[kNumMsm] = {};
+    cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};
+    cudaEvent_t ev_t[5] = {};
+    // the prove as a graph (witness already in z); kernels launched per replay
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    unsigned long long graph_kernels = 0;
+    // pinned staging: witness double buffer (pageable inputs) and results
+    void *pinned_wit[2] = {nullptr, nullptr};
+    cudaEvent_t ev_wit[2] = {nullptr, nullptr};
+    int wit_next = 0;
+    void *pinned_out = nullptr; // kOutBytes + 384 (blinding)
+    cudaStream_t main() const { return st[kMsmH]; }
+    ~ProveSlot();
+};
 
 } // namespace nkr
 
@@ -36,35 +68,36 @@ struct nkr_b200_key {
     nkr::CsrDevice mat[3];
     nkr::NttTables ntt;
     nkr::MsmBases bases[nkr::kNumMsm];
-    // digit sorts of the witness: one per distinct support among the 4 witness MSMs
-    // (B1 and B2 always share one); sort g runs on the stream of MSM sort_stream[g]
-    nkr::MsmSort sort_w[4];
+    // witness MSMs with identical supports share a digit sort: MSM k uses sort
+    // sort_of[k], which runs on the stream of MSM sort_stream[g]
     int n_sorts = 0;
     int sort_of[nkr::kNumMsm] = {};
     int sort_stream[4] = {};
-    nkr::MsmSort sort_h;               // digit sort of H
-    nkr::MsmAcc acc[nkr::kNumMsm];
-    nkr::DevBuf z, az, bz, cz, h;
-    nkr::DevBuf out;      // 4 G1 + 1 G2 results, libff Jacobian layout (96 * 4 + 192 B)
     nkr::DevBuf pk_const; // alpha_g1, beta_g1, delta_g1 (G1 affine) and beta_g2, delta_g2 (G2 affine)
     nkr::DevBuf blind_io; // r, s in; proof out
-    cudaStream_t st[nkr::kNumMsm] = {};
-    cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[nkr::kNumMsm] = {};
-    cudaEvent_t ev_t[5] = {};
-    void *pinned_in = nullptr;  // witness staging (cols * 32 B)
-    void *pinned_out = nullptr; // results staging (576 B + proof)
+    std::vector<std::unique_ptr<nkr::ProveSlot>> slots; // slots[0]: nkr_b200_prove
+    uint64_t slot_bytes = 0;                            // device bytes of one slot
     nkr_b200_stage_times times{};
     bool have_times = false;
 };
 
 namespace nkr {
 
-// Issue one full prove on the key's streams, witness already in key->z.
-// Results land in key->out (device, Jacobian with arbitrary Z).  No host
-// synchronisation.
-int prove_issue(nkr_b200_key *key, bool timed);
-
+// Adds one prove slot to the key (device buffers, streams, pinned staging).
+int slot_add(nkr_b200_key *key);
+// Issue one full prove on a slot's streams, witness already in slot->z.
+// Results land in slot->out (device, Jacobian with arbitrary Z).  No host
+// synchronisation; with timed, events bracket the stages on the main stream.
+int prove_issue(nkr_b200_key *key, ProveSlot *slot, bool timed);
+// Captures prove_issue into the slot's graph (once).
+int slot_capture(nkr_b200_key *key, ProveSlot *slot);
+// Queues the witness upload (device, pinned or pageable host memory) on the
+// slot's main stream; pageable input goes through the slot's pinned double buffer.
+int slot_upload_witness(nkr_b200_key *key, ProveSlot *slot, const void *witness);
+// Replays the slot's graph on its main stream.
+int slot_launch(ProveSlot *slot);
 // Affine-normalise the 4 G1 + 1 G2 result points (576 B, libff layout) in place.
 void normalize_raw(void *raw576);
+void raw_from_bytes(const void *raw576, nkr_b200_raw_proof *res);
 
 } // namespace nkr

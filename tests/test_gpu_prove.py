@@ -115,6 +115,39 @@ def test_repeated_proves_and_batch_agree(ctx):
     be2.free()
 
 
+def test_batch_mix_equals_single_proves(ctx):
+    """A batch of 18 proofs over 4 keys of different kinds and sizes (up to 6 proofs
+    of one key, more than its 4 slots, with distinct witnesses) returns exactly the
+    raw proof each witness gives alone through the plain path."""
+    specs = [("poseidon", 4, 1, 6), ("sql-aggregate", 8, 2, 5), ("matmul", 5, 0, 3),
+             ("poseidon", 16, 2, 4)]
+    backends, wits = [], []
+    for j, (kind, param, dens, nwit) in enumerate(specs):
+        r1 = nk.generate(kind, param, dens, seed=100 + j)
+        toxic = O.random_fr(5, np.random.default_rng(200 + j))
+        pk, _ = nk.setup(ctx, r1, toxic)
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        backends.append(be)
+        # poseidon / sql circuits do not depend on the seed, only their witnesses do
+        ws = [nk.generate(kind, param, dens, seed=300 + 10 * j + i).witness for i in range(nwit)]
+        wits.append(ws)
+    single = [[bytes(be.prove(w)) for w in ws] for be, ws in zip(backends, wits)]
+    order = []
+    for i in range(max(len(w) for w in wits)):
+        for j in range(len(specs)):
+            if i < len(wits[j]):
+                order.append((j, i))
+    out = nk.prove_batch([backends[j] for j, _ in order], [wits[j][i] for j, i in order])
+    for (j, i), raw in zip(order, out):
+        assert bytes(raw) == single[j][i], f"key {j} witness {i}"
+    # a second batch reuses the captured graphs and slots
+    out2 = nk.prove_batch([backends[j] for j, _ in order], [wits[j][i] for j, i in order])
+    assert [bytes(r) for r in out2] == [bytes(r) for r in out]
+    for be in backends:
+        be.free()
+
+
 def test_prepare_rejects_bad_shapes(ctx):
     g, r1, pk = _golden_matmul4()
     be = nk.Backend(ctx)
