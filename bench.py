@@ -387,6 +387,263 @@ def run_b200(args):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# batched form: 64 proofs of uneven size, batched vs plain sequential
+# ---------------------------------------------------------------------------
+
+def batch_mix(count=64, seed=4):
+    """The uneven mix: matmul size 16..64 or poseidon count 64..2048 (log-uniform),
+    hybrid density, sizes and kinds drawn from one seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    mix = []
+    for i in range(count):
+        if rng.random() < 0.5:
+            mix.append(("matmul", int(rng.integers(16, 65)), 1, 10_000 + i))
+        else:
+            mix.append(("poseidon", int(2 ** rng.integers(6, 12)), 1, 10_000 + i))
+    return mix
+
+
+def _pinned_copy(torch, arr):
+    import numpy as np
+    t = torch.empty(arr.size, dtype=torch.int64, pin_memory=True)
+    t.numpy()[:] = np.ascontiguousarray(arr).reshape(-1).view(np.int64)
+    return t
+
+
+def _prepare_keys(ctx, nk, specs, key_of):
+    """One prepared key per distinct circuit (GPU setup with seeded toxic waste)."""
+    keys = {}
+    for spec in specs:
+        kid = key_of(spec)
+        if kid in keys:
+            continue
+        kind, param, dens, seed = spec
+        r1 = nk.generate(kind, param, dens, seed=seed)
+        pk, _ = nk.setup(ctx, r1, _seeded_toxic(seed))
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        keys[kid] = be
+    return keys
+
+
+def run_batch(args):
+    import torch
+    import nkr_b200 as nk
+    t_setup = time.perf_counter()
+    ctx = nk.Context(0)
+    mix = batch_mix()
+    # poseidon circuits depend only on the count; a matmul circuit on its seed
+    key_of = lambda s: (s[0], s[1]) if s[0] == "poseidon" else (s[0], s[1], s[3])  # noqa: E731
+    keys = _prepare_keys(ctx, nk, mix, key_of)
+    bes, pins, rows = [], [], []
+    for kind, param, dens, seed in mix:
+        r1 = nk.generate(kind, param, dens, seed=seed)
+        bes.append(keys[key_of((kind, param, dens, seed))])
+        pins.append(_pinned_copy(torch, r1.witness))
+        rows.append(r1.rows)
+    ptrs = [t.data_ptr() for t in pins]
+    setup_s = time.perf_counter() - t_setup
+    clocks = ClockSampler(0)
+    # warm-up: slots, graphs and the tuner's size classes
+    first = [bytes(be.prove(None, witness_ptr=p)) for be, p in zip(bes, ptrs)]
+    for _ in range(args.warmup):
+        out = nk.prove_batch(bes, witness_ptrs=ptrs)
+    assert [bytes(o) for o in out] == first, "batched proofs differ from the plain proves"
+    clocks.start()
+    seq, bat = [], []
+    launches0 = nk.launch_count()
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        got = [bytes(be.prove(None, witness_ptr=p)) for be, p in zip(bes, ptrs)]
+        seq.append(time.perf_counter() - t)
+        assert got == first
+        t = time.perf_counter()
+        out = nk.prove_batch(bes, witness_ptrs=ptrs)
+        bat.append(time.perf_counter() - t)
+        assert [bytes(o) for o in out] == first
+    launches = (nk.launch_count() - launches0) // max(args.steps, 1)
+    clk = clocks.stop()
+    n = len(mix)
+    seq_pps = n / statistics.median(seq)
+    bat_pps = n / statistics.median(bat)
+    hist = {}
+    for r in rows:
+        hist[f"2^{r.bit_length() - 1}"] = hist.get(f"2^{r.bit_length() - 1}", 0) + 1
+    line = {
+        "metric": "batched Groth16 proofs/s, 64 uneven proofs (bit-exact)", "value": round(bat_pps, 2),
+        "unit": "proofs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": "bn254 (u32 limbs, exact)",
+        "data": "synthetic (seeded circuits, witnesses and toxic waste)",
+        "config": {"workload": "64 proofs: matmul s in [16, 64] or poseidon count 2^6..2^11, "
+                               "hybrid density, seed 4", "domains": dict(sorted(hist.items())),
+                   "distinct_keys": len(keys), "witness": "pinned host memory, uploaded per proof"},
+        "plain_sequential": {"value": round(seq_pps, 2), "unit": "proofs/s",
+                             "path": "nkr_b200_prove one proof at a time (upload, prove, download)"},
+        "speedup_vs_plain": round(bat_pps / seq_pps, 3),
+        "e2e": {"value": round(bat_pps, 2), "unit": "proofs/s",
+                "h2d_bytes_per_step": sum(t.numel() * 8 for t in pins),
+                "d2h_bytes_per_step": 576 * n},
+        "gpu_launches": launches, "clocks": clk, "setup_s": round(setup_s, 1),
+        "key_device_gib": round(sum(be.device_bytes() for be in keys.values()) / 2**30, 2),
+    }
+    print(json.dumps(line))
+    for be in keys.values():
+        be.free()
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------
+# serving form: Poisson stream over 6 resident keys, server vs plain FIFO
+# ---------------------------------------------------------------------------
+
+SERVE_KEYS = [("matmul", 32, 0), ("matmul", 64, 0), ("poseidon", 256, 2), ("poseidon", 4096, 2),
+              ("sql-aggregate", 1 << 10, 2), ("sql-aggregate", 1 << 14, 2)]
+
+
+def _percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def run_serve(args):
+    import threading
+    import numpy as np
+    import torch
+    import nkr_b200 as nk
+    t_setup = time.perf_counter()
+    ctx = nk.Context(0)
+    keys = SERVE_KEYS[:args.serve_keys]
+    bes, wits = [], []
+    for j, (kind, param, dens) in enumerate(keys):
+        r1 = nk.generate(kind, param, dens, seed=20 + j)
+        pk, _ = nk.setup(ctx, r1, _seeded_toxic(20 + j))
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        del pk
+        bes.append(be)
+        # matmul circuits depend on their seed: one witness; the others take fresh ones
+        ws = [r1.witness] if kind == "matmul" else [
+            r1.witness, nk.generate(kind, param, dens, seed=40 + j).witness]
+        wits.append([_pinned_copy(torch, w) for w in ws])
+    setup_s = time.perf_counter() - t_setup
+    # plain service times per key (also the warm-up of slot 0 of every key)
+    expect, service = [], []
+    for be, ws in zip(bes, wits):
+        expect.append([bytes(be.prove(None, witness_ptr=w.data_ptr())) for w in ws])
+        t = time.perf_counter()
+        be.prove(None, witness_ptr=ws[0].data_ptr())
+        service.append(time.perf_counter() - t)
+    mean_s = sum(service) / len(service)
+    lam = args.serve_load / mean_s  # offered load as a fraction of the plain path's capacity
+    rng = np.random.default_rng(5)
+    n_req = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
+    which = rng.integers(0, len(keys), n_req)
+    wsel = [int(rng.integers(0, len(wits[k]))) for k in which]
+
+    def replay(submit, wait_all):
+        t0 = time.perf_counter()
+        handles = []
+        for i in range(n_req):
+            d = arrivals[i] - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            handles.append(submit(i, t0))
+        res = wait_all(handles)
+        return res, time.perf_counter() - t0
+
+    # plain arm: one request at a time in arrival order (FIFO), the same arrivals
+    def plain_arm():
+        done = [None] * n_req
+        q, cv = [], threading.Condition()
+
+        def worker():
+            for i in range(n_req):
+                with cv:
+                    while not q:
+                        cv.wait()
+                    j, t0 = q.pop(0)
+                k = which[j]
+                raw = bytes(bes[k].prove(None, witness_ptr=wits[k][wsel[j]].data_ptr()))
+                done[j] = (raw, (time.perf_counter() - t0 - arrivals[j]) * 1e3)
+        th = threading.Thread(target=worker)
+        th.start()
+
+        def submit(i, t0):
+            with cv:
+                q.append((i, t0))
+                cv.notify()
+            return i
+        res, wall = replay(submit, lambda h: (th.join(), done)[1])
+        return res, wall
+
+    def server_arm():
+        sv = nk.Server(ctx, max_inflight=args.serve_inflight, max_slots_per_key=4)
+        ids = [sv.add_key(be) for be in bes]
+
+        def submit(i, t0):
+            k = which[i]
+            return sv.submit(ids[k], witness_ptr=wits[k][wsel[i]].data_ptr())
+
+        def wait_all(handles):
+            out = []
+            for h in handles:
+                raw, lat, _ = sv.wait(h)
+                out.append((bytes(raw), lat))
+            return out
+        res, wall = replay(submit, wait_all)
+        slots = [sv.slots(i) for i in ids]
+        sv.close()
+        return res, wall, slots
+
+    clocks = ClockSampler(0)
+    # server warm-up: slots and graphs of every key
+    server_arm_warm = nk.Server(ctx, max_inflight=args.serve_inflight, max_slots_per_key=4)
+    wids = [server_arm_warm.add_key(be) for be in bes]
+    for _ in range(2):
+        hs = [server_arm_warm.submit(wids[k], witness_ptr=wits[k][0].data_ptr())
+              for k in range(len(keys)) for _ in range(4)]
+        for h in hs:
+            server_arm_warm.wait(h)
+    server_arm_warm.close()
+    clocks.start()
+    launches0 = nk.launch_count()
+    plain, plain_wall = plain_arm()
+    srv, srv_wall, slots = server_arm()
+    clk = clocks.stop()
+    ok = all(plain[i][0] == expect[which[i]][wsel[i]] and srv[i][0] == expect[which[i]][wsel[i]]
+             for i in range(n_req))
+    lat_p = [x[1] for x in plain]
+    lat_s = [x[1] for x in srv]
+    line = {
+        "metric": "served Groth16 proofs/s and latency, Poisson stream over 6 resident keys",
+        "value": round(n_req / srv_wall, 2), "unit": "proofs/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "bn254 (u32 limbs, exact)", "bit_exact": ok,
+        "data": "synthetic (seeded circuits, witnesses, toxic waste and arrivals)",
+        "config": {"workload": "keys " + ", ".join(f"{k} {p}" for k, p, _ in keys),
+                   "requests": n_req, "offered_load": args.serve_load,
+                   "arrival_rate_per_s": round(lam, 2),
+                   "plain_service_ms": [round(x * 1e3, 2) for x in service],
+                   "max_inflight": args.serve_inflight, "slots_used": slots},
+        "server": {"proofs_per_s": round(n_req / srv_wall, 2),
+                   "p50_ms": round(_percentile(lat_s, 50), 2), "p99_ms": round(_percentile(lat_s, 99), 2)},
+        "plain_fifo": {"proofs_per_s": round(n_req / plain_wall, 2),
+                       "p50_ms": round(_percentile(lat_p, 50), 2),
+                       "p99_ms": round(_percentile(lat_p, 99), 2)},
+        "gpu_launches": nk.launch_count() - launches0, "clocks": clk, "setup_s": round(setup_s, 1),
+        "key_device_gib": round(sum(be.device_bytes() for be in bes) / 2**30, 2),
+    }
+    print(json.dumps(line))
+    for be in bes:
+        be.free()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,9 +652,20 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="poseidon2048", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="prove", choices=["prove", "batch", "serve"],
+                    help="prove: the 2^20 prove (default line); batch: 64 uneven proofs batched vs "
+                         "plain; serve: Poisson requests over resident keys, server vs plain FIFO")
+    ap.add_argument("--serve-keys", type=int, default=6)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--serve-inflight", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "batch":
+        run_batch(args)
+    elif args.mode == "serve":
+        run_serve(args)
     else:
         run_b200(args)
 

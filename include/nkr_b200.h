@@ -131,6 +131,27 @@ int nkr_b200_key_stage_times(const nkr_b200_key *key, nkr_b200_stage_times *out)
 int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
                          nkr_b200_raw_proof *out);
 
+/* ---- request server (continuous batching over resident keys) -------------
+ * No counterpart in the reference, which proves one request per process
+ * (app/prove.cpp:70-88).  A scheduler thread admits waiting requests, oldest
+ * first, onto free prove slots of their key (adding slots while free HBM allows,
+ * up to max_slots_per_key per key and max_inflight in total) and replays each
+ * slot's captured prove graph, so requests of different circuits overlap on the
+ * GPU.  The witness memory of a request must stay valid until its wait returns.
+ * A key added to a server is proved only through that server while it runs. */
+typedef struct nkr_b200_server nkr_b200_server;
+int nkr_b200_server_create(nkr_b200_ctx *ctx, int max_inflight, int max_slots_per_key,
+                           nkr_b200_server **out);
+int nkr_b200_server_add_key(nkr_b200_server *server, nkr_b200_key *key, int *key_id);
+int nkr_b200_server_submit(nkr_b200_server *server, int key_id, const void *witness,
+                           uint64_t *request_id);
+/* Blocks until the request is done; latency = submit to result on the host, queue =
+ * submit to start on the GPU (milliseconds; either pointer may be NULL). */
+int nkr_b200_server_wait(nkr_b200_server *server, uint64_t request_id, nkr_b200_raw_proof *out,
+                         double *latency_ms, double *queue_ms);
+int nkr_b200_server_slots(nkr_b200_server *server, int key_id, int *slots);
+void nkr_b200_server_destroy(nkr_b200_server *server);
+
 /* ---- operator-level entry points (operators/cuda/include/nkr/operators/cuda.hpp) */
 
 /* libfqfft radix-2 domain ops on n = 2^k Fr values (host buffer, in place):
@@ -164,6 +185,17 @@ int nkr_b200_msm_g1(nkr_b200_ctx *ctx, const void *bases, const void *scalars, u
                     void *out);
 int nkr_b200_msm_g2(nkr_b200_ctx *ctx, const void *bases, const void *scalars, uint64_t n,
                     void *out);
+
+/* MSM window autotuner (on by default; environment NKR_B200_AUTOTUNE=0 turns it
+ * off).  The window width of every resident MSM (prepare, msm_bases_create) is
+ * measured once per power-of-two size class on this device: the cost model's
+ * width and its neighbours are timed on synthetic bases and the fastest kept.
+ * nkr_b200_tune_msm returns (and, if needed, measures) the width for n points and
+ * the measured MSM time at that size class (0 when the size is not measured).
+ * Replaces choose_window_bits (backends/cuda/src/groth16_backend.cu:17-25: 8, 11
+ * or 13 bits by size), which has no tuner. */
+int nkr_b200_set_autotune(nkr_b200_ctx *ctx, int enable);
+int nkr_b200_tune_msm(nkr_b200_ctx *ctx, uint64_t n, int *window_bits, float *ms);
 
 /* Resident-bases MSM (the prove path's form): bases uploaded and expanded once
  * into per-window copies, then any number of MSMs with new scalars. */

@@ -313,7 +313,10 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     NKR_REQUIRE(out && (n == 0 || bases), "null argument");
     auto h = std::make_unique<nkr_b200_msm_bases>();
     h->ctx = ctx;
-    NKR_TRY(msm_bases_build_support(h->bases, group, bases, n, true, ctx->stream));
+    std::vector<uint32_t> idx = msm_support(group, bases, n);
+    int c = 0;
+    NKR_TRY(tuned_window_bits(ctx, idx.size(), &c));
+    NKR_TRY(msm_bases_build_support(h->bases, group, bases, n, std::move(idx), true, c, ctx->stream));
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
     NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[0]));
     NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[1]));
@@ -393,6 +396,29 @@ void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
     for (auto &e : b->scratch.acc.ev_acc)
         if (e) cudaEventDestroy(e);
     delete b;
+}
+
+int nkr_b200_set_autotune(nkr_b200_ctx *ctx, int enable)
+{
+    NKR_REQUIRE(ctx, "null context");
+    ctx->autotune = enable != 0;
+    return NKR_B200_OK;
+}
+
+int nkr_b200_tune_msm(nkr_b200_ctx *ctx, uint64_t n, int *window_bits, float *ms)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(window_bits, "null argument");
+    int c = 0;
+    NKR_TRY(tuned_window_bits(ctx, n, &c));
+    if (c == 0) c = msm_shape(n, true, 1).c;
+    *window_bits = c;
+    if (ms) {
+        int lg = 0;
+        while ((uint64_t(1) << lg) < n) ++lg;
+        *ms = lg < 33 ? ctx->msm_window_ms[lg] : 0.f;
+    }
+    return NKR_B200_OK;
 }
 
 int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const void *b, void *out,

@@ -647,11 +647,8 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
     return NKR_B200_OK;
 }
 
-int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n, bool folded,
-                            cudaStream_t st)
+std::vector<uint32_t> msm_support(int group, const void *jac_host, uint64_t n)
 {
-    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
-    NKR_REQUIRE(n < (uint64_t(1) << 32), "support indices are 32-bit");
     const size_t jac_sz = group == 1 ? 96 : 192;
     const size_t z_off = jac_sz / 3 * 2, z_sz = jac_sz / 3;
     const uint8_t *src = static_cast<const uint8_t *>(jac_host);
@@ -668,10 +665,23 @@ int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64
         if (!zero) idx.push_back(uint32_t(i));
     }
     if (idx.empty() && n) idx.push_back(0); // an all-infinity query still has one (zero) term
+    return idx;
+}
+
+int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n,
+                            std::vector<uint32_t> idx, bool folded, int c_override, cudaStream_t st)
+{
+    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
+    NKR_REQUIRE(n < (uint64_t(1) << 32), "support indices are 32-bit");
+    NKR_REQUIRE(idx.size() <= n && (n == 0 || !idx.empty()), "support index list does not fit the bases");
+    const size_t jac_sz = group == 1 ? 96 : 192;
+    const uint8_t *src = static_cast<const uint8_t *>(jac_host);
     std::vector<uint8_t> packed(std::max<size_t>(idx.size(), 1) * jac_sz);
-    for (size_t j = 0; j < idx.size(); ++j)
+    for (size_t j = 0; j < idx.size(); ++j) {
+        NKR_REQUIRE(idx[j] < n, "support index out of range");
         std::memcpy(packed.data() + j * jac_sz, src + uint64_t(idx[j]) * jac_sz, jac_sz);
-    NKR_TRY(msm_bases_build(b, group, packed.data(), false, idx.size(), folded, 0, false, st));
+    }
+    NKR_TRY(msm_bases_build(b, group, packed.data(), false, idx.size(), folded, c_override, false, st));
     b.n_full = n;
     NKR_TRY(b.support.alloc(std::max<size_t>(idx.size(), 1) * 4, "msm support indices"));
     if (!idx.empty())

@@ -116,11 +116,13 @@ struct MsmBases {
 // scalars held in bit-reversed order pair with their own bases.
 int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device, uint64_t n,
                     bool folded, int c_override, bool bitrev, cudaStream_t st);
-// Resident bases of the finite points among n host bases (libff Jacobian, Z = 0
-// is infinity); the scalars of this MSM are indexed by original point index
-// through gather().  Keeps one (infinite) point when all n are infinite.
-int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n, bool folded,
-                            cudaStream_t st);
+// Indices of the finite points among n host bases (libff Jacobian, Z = 0 is
+// infinity); one index (0) when all n are infinite.
+std::vector<uint32_t> msm_support(int group, const void *jac_host, uint64_t n);
+// Resident bases of the points idx (from msm_support) of n host bases; the
+// scalars of this MSM are indexed by original point index through gather().
+int msm_bases_build_support(MsmBases &b, int group, const void *jac_host, uint64_t n,
+                            std::vector<uint32_t> idx, bool folded, int c_override, cudaStream_t st);
 
 // Normalise n libff-layout Jacobian points (device) into affine (device).
 int jacobian_to_affine(int group, const void *jac, void *aff, uint64_t n, cudaStream_t st);

@@ -347,11 +347,20 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
     NKR_PREP(ntt_tables_build(key->ntt, logn, st));
     // proving key: normalise (hazard: CPU-setup keys are unnormalised Jacobian), fold
     // windows; witness queries keep only their finite points (variables present in the matrix)
-    NKR_PREP(msm_bases_build_support(key->bases[kMsmA], 1, pk->a_query, c->cols, true, st));
-    NKR_PREP(msm_bases_build_support(key->bases[kMsmB1], 1, pk->b_g1_query, c->cols, true, st));
-    NKR_PREP(msm_bases_build_support(key->bases[kMsmL], 1, pk->l_query, c->cols, true, st));
-    NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, 0, true, st));
-    NKR_PREP(msm_bases_build_support(key->bases[kMsmB2], 2, pk->b_g2_query, c->cols, true, st));
+    // window widths from the autotuner (per support size; 0 = cost model)
+    const void *wq[4] = {pk->a_query, pk->b_g1_query, pk->l_query, pk->b_g2_query};
+    const int wk[4] = {kMsmA, kMsmB1, kMsmL, kMsmB2};
+    for (int j = 0; j < 4; ++j) {
+        const int group = wk[j] == kMsmB2 ? 2 : 1;
+        std::vector<uint32_t> idx = msm_support(group, wq[j], c->cols);
+        int cw = 0;
+        NKR_PREP(tuned_window_bits(ctx, idx.size(), &cw));
+        NKR_PREP(msm_bases_build_support(key->bases[wk[j]], group, wq[j], c->cols, std::move(idx), true,
+                                         cw, st));
+    }
+    int ch = 0;
+    NKR_PREP(tuned_window_bits(ctx, c->rows, &ch));
+    NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, ch, true, st));
     // MSMs with the same support (and so the same window shape) share a digit sort
     key->n_sorts = 0;
     for (int k : kWitnessOrder) {

@@ -30,7 +30,19 @@ struct nkr_b200_ctx {
     int device = 0;
     int sm_count = 0;
     cudaStream_t stream = nullptr; // operator-level calls
+    // MSM window autotuner: measured best window bits per log2 point count
+    // (0 = not measured yet); off: the cost model of msm_shape decides
+    bool autotune = true;
+    int msm_window[33] = {};
+    float msm_window_ms[33] = {};
 };
+
+namespace nkr {
+// Window bits for an MSM of n points: measured once per power-of-two size class
+// on this device when autotuning is on (synthetic bases, uniform scalars),
+// else 0 (the cost model).  Sizes above 2^22 take the 2^22 offset from the model.
+int tuned_window_bits(nkr_b200_ctx *ctx, uint64_t n, int *c);
+} // namespace nkr
 
 namespace nkr {
 

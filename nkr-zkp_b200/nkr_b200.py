@@ -25,6 +25,10 @@ if not os.path.exists(LIB_PATH):
         f"{LIB_PATH} is missing: build it with `python nkr-zkp_b200/build.py` "
         "(there is no CPU fallback for the B200 backend)")
 
+# more hardware work queues than the default 8, so the many streams of concurrent
+# prove slots do not alias onto a few queues (read when the CUDA context is created)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 _lib = ctypes.CDLL(LIB_PATH)
 
 OK, EINVAL, ECUDA, ENOMEM, ENODEV, ETIMEOUT, EBUSY = range(7)
@@ -82,6 +86,17 @@ _SIGS = {
     "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
                                             ctypes.POINTER(RawProofC)]),
     "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
+    "nkr_b200_server_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
+    "nkr_b200_server_add_key": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_int)]),
+    "nkr_b200_server_submit": (ctypes.c_int, [_VP, ctypes.c_int, _VP, ctypes.POINTER(_U64)]),
+    "nkr_b200_server_wait": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(RawProofC),
+                                            ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]),
+    "nkr_b200_server_slots": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "nkr_b200_server_destroy": (None, [_VP]),
+    "nkr_b200_set_autotune": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "nkr_b200_tune_msm": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_float)]),
     "nkr_b200_ntt_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _U64, _VP]),
     "nkr_b200_spmv": (ctypes.c_int, [_VP, _U64, _U64, _VP, _VP, _VP, _VP, _VP]),
     "nkr_b200_msm_g1": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
@@ -285,6 +300,16 @@ class Context:
                f"group_op {group} {op}")
         return out
 
+    def set_autotune(self, enable):
+        _check(_lib.nkr_b200_set_autotune(self.h, int(bool(enable))), "set_autotune")
+
+    def tune_msm(self, n):
+        """(window bits, measured ms at that size class) for an MSM of n points."""
+        c = ctypes.c_int()
+        ms = ctypes.c_float()
+        _check(_lib.nkr_b200_tune_msm(self.h, n, ctypes.byref(c), ctypes.byref(ms)), "tune_msm")
+        return c.value, ms.value
+
     def bench_mul(self, field):
         rate, ms = ctypes.c_double(), ctypes.c_double()
         _check(_lib.nkr_b200_bench_mul(self.h, field, ctypes.byref(rate), ctypes.byref(ms)),
@@ -449,11 +474,67 @@ def setup(ctx, r1cs, toxic):
     return pk, vk
 
 
-def prove_batch(backends, witnesses):
+def prove_batch(backends, witnesses=None, witness_ptrs=None):
+    """Batched prove (nkr_b200_prove_batch): numpy witnesses, or raw pointers
+    (pinned host or device memory) in witness_ptrs."""
     n = len(backends)
     keys = (_VP * n)(*[b.key for b in backends])
-    ws = [_fr(w) for w in witnesses]
-    wp = (_VP * n)(*[w.ctypes.data for w in ws])
+    if witness_ptrs is None:
+        ws = [_fr(w) for w in witnesses]
+        witness_ptrs = [w.ctypes.data for w in ws]
+    wp = (_VP * n)(*witness_ptrs)
     out = (RawProofC * n)()
     _check(_lib.nkr_b200_prove_batch(keys, wp, n, out), "prove_batch")
     return list(out)
+
+
+class Server:
+    """Request server (nkr_b200_server_*): continuous batching over resident keys.
+    Witness arrays are kept referenced until their request is waited for."""
+
+    def __init__(self, ctx, max_inflight=8, max_slots_per_key=4):
+        h = _VP()
+        _check(_lib.nkr_b200_server_create(ctx.h, max_inflight, max_slots_per_key, ctypes.byref(h)),
+               "server_create")
+        self.h = h
+        self._pending = {}
+
+    def add_key(self, backend):
+        kid = ctypes.c_int()
+        _check(_lib.nkr_b200_server_add_key(self.h, backend.key, ctypes.byref(kid)), "server_add_key")
+        return kid.value
+
+    def submit(self, key_id, witness=None, witness_ptr=None):
+        keep = None
+        if witness_ptr is None:
+            keep = _fr(witness)
+            witness_ptr = keep.ctypes.data
+        rid = _U64()
+        _check(_lib.nkr_b200_server_submit(self.h, key_id, witness_ptr, ctypes.byref(rid)), "server_submit")
+        self._pending[rid.value] = keep
+        return rid.value
+
+    def wait(self, rid):
+        """(RawProofC, latency ms, queue ms)"""
+        raw = RawProofC()
+        lat, q = ctypes.c_double(), ctypes.c_double()
+        st = _lib.nkr_b200_server_wait(self.h, rid, ctypes.byref(raw), ctypes.byref(lat), ctypes.byref(q))
+        self._pending.pop(rid, None)
+        _check(st, "server_wait")
+        return raw, lat.value, q.value
+
+    def slots(self, key_id):
+        n = ctypes.c_int()
+        _check(_lib.nkr_b200_server_slots(self.h, key_id, ctypes.byref(n)), "server_slots")
+        return n.value
+
+    def close(self):
+        if self.h:
+            _lib.nkr_b200_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -86,6 +86,27 @@ def test_msm_mostly_and_all_infinity_bases(ctx, orc, rng, group):
     _check(ctx, orc, group, aff, sc, folded=True)
 
 
+def test_autotuned_window_matches_model_window(ctx, orc, rng):
+    """The tuner picks a window per size class on this GPU; any window gives the
+    same canonical result, so tuned and cost-model MSMs agree with the oracle."""
+    n = 1 << 14
+    c, ms = ctx.tune_msm(n)
+    assert 6 <= c <= 22 and ms > 0
+    assert ctx.tune_msm(n - 1000) == (c, ms)  # same size class, measured once
+    model = nk.Context(0)
+    model.set_autotune(False)
+    aff = _points(orc, 1, n, rng, distinct=512)
+    sc = O.random_fr(n, rng)
+    jac = O.affine_to_jac(1, aff)
+    want = O.affine_to_jac(1, orc.msm(1, aff, sc))[0]
+    for cx in (ctx, model):
+        b = nk.MsmBases(cx, 1, jac)
+        got, _ = b.run(sc)
+        assert np.array_equal(got, want)
+        b.free()
+    model.close()
+
+
 @pytest.mark.parametrize("folded", [False, True])
 def test_msm_all_zero_scalars_is_infinity(ctx, orc, rng, folded):
     aff = _points(orc, 1, 50, rng)

@@ -1,0 +1,84 @@
+"""Request server (continuous batching over resident keys): every result equals
+the raw proof the same witness gives alone through the plain path, whether the
+request runs alone on an idle server or in a mix of circuits with requests of
+several keys in flight, submitted from several host threads."""
+import threading
+
+import numpy as np
+import pytest
+
+import nkr_b200 as nk
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [("poseidon", 4, 1, 5), ("sql-aggregate", 8, 2, 4), ("matmul", 5, 0, 1), ("poseidon", 16, 2, 3)]
+
+
+@pytest.fixture(scope="module")
+def keyset(ctx):
+    backends, wits = [], []
+    for j, (kind, param, dens, nwit) in enumerate(SPECS):
+        r1 = nk.generate(kind, param, dens, seed=500 + j)
+        pk, _ = nk.setup(ctx, r1, O.random_fr(5, np.random.default_rng(600 + j)))
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        backends.append(be)
+        wits.append([nk.generate(kind, param, dens, seed=700 + 10 * j + i).witness for i in range(nwit)])
+    single = [[bytes(be.prove(w)) for w in ws] for be, ws in zip(backends, wits)]
+    yield backends, wits, single
+    for be in backends:
+        be.free()
+
+
+def test_alone_and_in_mix_equal_plain_proves(ctx, keyset):
+    backends, wits, single = keyset
+    sv = nk.Server(ctx, max_inflight=6, max_slots_per_key=3)
+    ids = [sv.add_key(be) for be in backends]
+    # alone: one request on an idle server
+    rid = sv.submit(ids[1], wits[1][0])
+    raw, lat, q = sv.wait(rid)
+    assert bytes(raw) == single[1][0] and lat >= q >= 0
+    # mix: all requests submitted back to back, interleaved across keys
+    order = [(j, i) for i in range(5) for j in range(len(SPECS)) if i < len(wits[j])]
+    rids = [(j, i, sv.submit(ids[j], wits[j][i])) for j, i in order]
+    for j, i, r in rids:
+        raw, lat, q = sv.wait(r)
+        assert bytes(raw) == single[j][i], f"key {j} witness {i}"
+    assert 1 <= sv.slots(ids[0]) <= 3
+    sv.close()
+
+
+def test_submitters_on_several_threads(ctx, keyset):
+    backends, wits, single = keyset
+    sv = nk.Server(ctx, max_inflight=8, max_slots_per_key=2)
+    ids = [sv.add_key(be) for be in backends]
+    errors = []
+
+    def client(j):
+        try:
+            for rep in range(2):
+                rs = [(i, sv.submit(ids[j], w)) for i, w in enumerate(wits[j])]
+                for i, r in rs:
+                    raw, _, _ = sv.wait(r)
+                    if bytes(raw) != single[j][i]:
+                        errors.append((j, i, rep))
+        except Exception as e:  # surfaced below
+            errors.append(repr(e))
+
+    ts = [threading.Thread(target=client, args=(j,)) for j in range(len(SPECS))]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    sv.close()
+    assert not errors, errors
+
+
+def test_rejects_unknown_key_and_request(ctx, keyset):
+    sv = nk.Server(ctx)
+    with pytest.raises(nk.B200Error, match="unknown key"):
+        sv.submit(3, keyset[1][0][0])
+    with pytest.raises(nk.B200Error, match="unknown request"):
+        sv.wait(12345)
+    sv.close()
