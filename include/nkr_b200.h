@@ -222,7 +222,9 @@ uint64_t nkr_b200_launch_count(void);
 /* ---- field / group primitives (tests and microbenchmarks) ------------------ */
 
 /* Elementwise field op over n pairs (host buffers): field 0 Fr, 1 Fq, 2 Fq2;
- * op 0 mul, 1 add, 2 sub, 3 sqr, 4 inverse, 5 to_mont, 6 from_mont. */
+ * op 0 mul, 1 add, 2 sub, 3 sqr, 4 inverse, 5 to_mont, 6 from_mont.  Fields 3
+ * (Fq) and 4 (Fq2) run ops 0..3 and 4 = negation in the MSM's FP64-limb
+ * arithmetic (same inputs and outputs as fields 1 and 2). */
 int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const void *b,
                       void *out, uint64_t n);
 /* Elementwise group op: group 1 G1, 2 G2; inputs affine-normalised Jacobian layout.

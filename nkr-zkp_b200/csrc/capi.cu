@@ -426,7 +426,8 @@ int nkr_b200_field_op(nkr_b200_ctx *ctx, int field, int op, const void *a, const
 {
     NKR_TRY(ctx_check(ctx));
     NKR_REQUIRE(a && out, "null argument");
-    const size_t esz = field == 2 ? 64 : 32;
+    NKR_REQUIRE(field >= 0 && field <= 4, "field %d unknown", field);
+    const size_t esz = (field == 2 || field == 4) ? 64 : 32; // Fq2 elements are 64 B
     cudaStream_t st = ctx->stream;
     DevBuf da, db, dout;
     NKR_TRY(da.alloc(std::max<uint64_t>(n, 1) * esz, "field op a"));

@@ -1,0 +1,322 @@
+// Fq in five 52-bit limbs with products on the double-precision FMA pipe.
+//
+// The Montgomery product of field.cuh is bound by the integer multiply (IMAD)
+// pipe and, for one warp alone, by its long carry chains (about a microsecond
+// of latency per product).  B200 also has a full-rate FP64 pipe, and a double
+// FMA computes a 52 x 52-bit limb product exactly when the high half is taken
+// with round toward zero against a 2^104 offset and the low half as the exact
+// remainder (Emmart, Zheng and Weems, "Faster modular exponentiation using
+// double precision floating point arithmetic on the GPU", ARITH 2018):
+//     h = fma_rz(a, b, 2^104)              = 2^104 + floor(a b / 2^52) 2^52
+//     l = fma(a, b, (2^104 + 2^52) - h)    = 2^52 + (a b mod 2^52)
+// Both results hold their integer in the mantissa, so their bit patterns minus
+// the offsets' bit patterns are the integers; the 25 limb products of a x b
+// are independent, columns are summed as 64-bit integers and the offsets are
+// removed once per column.  The reduction is word-serial Montgomery with
+// 52-bit words (q = t * (-p^-1) mod 2^52, also by FMA).
+//
+// Representation: limbs are uint64 integers < 2^52, values canonical (< p),
+// Montgomery form with R' = 2^260.  In memory these values are stored in the
+// 8 x 32-bit layout of Fq (to52 / from52 only move bits); the MSM keeps all of
+// its buffers in the R' domain and converts at entry (bases) and exit (result).
+#pragma once
+
+#include <cstdint>
+
+#include "field.cuh"
+
+namespace nkr {
+
+struct Fq52 {
+    uint64_t l[5];
+    __device__ __forceinline__ static Fq52 zero() { return {{0, 0, 0, 0, 0}}; }
+    // 2^260 mod p
+    __device__ __forceinline__ static Fq52 one()
+    {
+        return {{0x20880f6fce4b4ull, 0x49baa989a8455ull, 0x18f014a498908ull, 0x724f85a9201d8ull,
+                 0x1f16424e1bb7ull}};
+    }
+    __device__ __forceinline__ bool is_zero() const
+    {
+        return (l[0] | l[1] | l[2] | l[3] | l[4]) == 0;
+    }
+    __device__ __forceinline__ bool operator==(const Fq52 &o) const
+    {
+        return ((l[0] ^ o.l[0]) | (l[1] ^ o.l[1]) | (l[2] ^ o.l[2]) | (l[3] ^ o.l[3]) |
+                (l[4] ^ o.l[4])) == 0;
+    }
+    __device__ __forceinline__ bool operator!=(const Fq52 &o) const { return !(*this == o); }
+};
+
+namespace f52 {
+
+constexpr uint64_t kMask = (uint64_t(1) << 52) - 1;
+constexpr uint64_t kBias52 = 0x4330000000000000ull;  // bit pattern of 2^52
+constexpr uint64_t kBias104 = 0x4670000000000000ull; // bit pattern of 2^104
+// p in 52-bit limbs and -p^-1 mod 2^52
+__host__ __device__ constexpr uint64_t p_limb(int k)
+{
+    return k == 0 ? 0x8c16d87cfd47ull
+           : k == 1 ? 0x916871ca8d3c2ull
+           : k == 2 ? 0x181585d97816aull
+           : k == 3 ? 0xa029b85045b68ull
+                    : 0x30644e72e131ull;
+}
+constexpr uint64_t kPinv = 0x20782e4866389ull;
+
+__device__ __forceinline__ double to_double(uint64_t v) // v < 2^52, exact
+{
+    return __longlong_as_double(static_cast<long long>(kBias52 | v)) - 0x1p52;
+}
+
+// a b = hi 2^52 + lo for integers a, b < 2^52 held in doubles; returns the
+// offset bit patterns (kBias52 + lo, kBias104 + hi)
+__device__ __forceinline__ void mul_wide(double a, double b, uint64_t &lo_b, uint64_t &hi_b)
+{
+    const double h = __fma_rz(a, b, 0x1p104);
+    const double c = (0x1p104 + 0x1p52) - h;
+    const double l = __fma_rn(a, b, c);
+    hi_b = static_cast<uint64_t>(__double_as_longlong(h));
+    lo_b = static_cast<uint64_t>(__double_as_longlong(l));
+}
+
+// s (five 52-bit limbs, value < 2p) minus p when s >= p
+__device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
+{
+    uint64_t d[5];
+    int64_t borrow = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int64_t t = int64_t(s[k]) - int64_t(p_limb(k)) + borrow;
+        d[k] = uint64_t(t) & kMask;
+        borrow = t >> 52;
+    }
+    if (borrow == 0) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s[k] = d[k];
+    }
+}
+
+} // namespace f52
+
+#ifdef NKR_FIELD_MUL_OUTLINE
+#define NKR_MUL52_ATTR __noinline__
+#else
+#define NKR_MUL52_ATTR __forceinline__
+#endif
+
+// a b 2^-260 mod p, canonical; needs a b < 2^260 p (true for a, b < 4p)
+__device__ NKR_MUL52_ATTR Fq52 mul52(const Fq52 &a, const Fq52 &b)
+{
+    using namespace f52;
+    double ad[5], bd[5], pd[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        ad[i] = to_double(a.l[i]);
+        bd[i] = to_double(b.l[i]);
+        pd[i] = double(p_limb(i)); // exact, folded at compile time
+    }
+    uint64_t C[10];
+    uint64_t bias[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        C[k] = 0;
+        bias[k] = 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            uint64_t lo, hi;
+            mul_wide(ad[i], bd[j], lo, hi);
+            C[i + j] += lo;
+            bias[i + j] += kBias52;
+            C[i + j + 1] += hi;
+            bias[i + j + 1] += kBias104;
+        }
+    const double pinv = double(kPinv);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        uint64_t t = C[i] - bias[i]; // the column's integer value
+        uint64_t qlo, qhi;
+        mul_wide(to_double(t & kMask), pinv, qlo, qhi);
+        const double q = __longlong_as_double(static_cast<long long>(qlo)) - 0x1p52;
+        uint64_t lo, hi;
+        mul_wide(q, pd[0], lo, hi);
+        t += lo - kBias52; // now 0 mod 2^52
+        C[i + 1] += hi + (t >> 52);
+        bias[i + 1] += kBias104;
+#pragma unroll
+        for (int j = 1; j < 5; ++j) {
+            mul_wide(q, pd[j], lo, hi);
+            C[i + j] += lo;
+            bias[i + j] += kBias52;
+            if (i + j + 1 < 10) {
+                C[i + j + 1] += hi;
+                bias[i + j + 1] += kBias104;
+            }
+        }
+    }
+    Fq52 r;
+    uint64_t carry = 0;
+#pragma unroll
+    for (int k = 5; k < 10; ++k) {
+        const uint64_t v = C[k] - bias[k] + carry;
+        r.l[k - 5] = v & kMask;
+        carry = v >> 52;
+    }
+    sub_p_if_ge(r.l); // the result is below 2p
+    return r;
+}
+
+__device__ __forceinline__ Fq52 operator*(const Fq52 &a, const Fq52 &b) { return mul52(a, b); }
+__device__ __forceinline__ Fq52 sqr(const Fq52 &a) { return mul52(a, a); }
+
+__device__ __forceinline__ Fq52 operator+(const Fq52 &a, const Fq52 &b)
+{
+    Fq52 r;
+    uint64_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const uint64_t t = a.l[k] + b.l[k] + c;
+        r.l[k] = t & f52::kMask;
+        c = t >> 52;
+    }
+    f52::sub_p_if_ge(r.l);
+    return r;
+}
+
+__device__ __forceinline__ Fq52 operator-(const Fq52 &a, const Fq52 &b)
+{
+    Fq52 r;
+    int64_t br = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int64_t t = int64_t(a.l[k]) - int64_t(b.l[k]) + br;
+        r.l[k] = uint64_t(t) & f52::kMask;
+        br = t >> 52;
+    }
+    if (br) { // a < b: add p back
+        uint64_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const uint64_t t = r.l[k] + f52::p_limb(k) + c;
+            r.l[k] = t & f52::kMask;
+            c = t >> 52;
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ Fq52 neg(const Fq52 &a) { return Fq52::zero() - a; }
+__device__ __forceinline__ Fq52 dbl(const Fq52 &a) { return a + a; }
+
+// Fq2 = Fq[u] / (u^2 + 1) over Fq52 (Karatsuba, as Fq2 in field.cuh)
+struct Fq2x52 {
+    Fq52 c0, c1;
+    __device__ __forceinline__ static Fq2x52 zero() { return {Fq52::zero(), Fq52::zero()}; }
+    __device__ __forceinline__ static Fq2x52 one() { return {Fq52::one(), Fq52::zero()}; }
+    __device__ __forceinline__ bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+    __device__ __forceinline__ bool operator==(const Fq2x52 &o) const
+    {
+        return c0 == o.c0 && c1 == o.c1;
+    }
+    __device__ __forceinline__ bool operator!=(const Fq2x52 &o) const { return !(*this == o); }
+};
+
+__device__ __forceinline__ Fq2x52 operator+(const Fq2x52 &a, const Fq2x52 &b)
+{
+    return {a.c0 + b.c0, a.c1 + b.c1};
+}
+__device__ __forceinline__ Fq2x52 operator-(const Fq2x52 &a, const Fq2x52 &b)
+{
+    return {a.c0 - b.c0, a.c1 - b.c1};
+}
+__device__ __forceinline__ Fq2x52 neg(const Fq2x52 &a) { return {neg(a.c0), neg(a.c1)}; }
+__device__ __forceinline__ Fq2x52 dbl(const Fq2x52 &a) { return {dbl(a.c0), dbl(a.c1)}; }
+__device__ __forceinline__ Fq2x52 operator*(const Fq2x52 &a, const Fq2x52 &b)
+{
+    const Fq52 v0 = a.c0 * b.c0;
+    const Fq52 v1 = a.c1 * b.c1;
+    const Fq52 s = (a.c0 + a.c1) * (b.c0 + b.c1);
+    return {v0 - v1, s - v0 - v1};
+}
+__device__ __forceinline__ Fq2x52 sqr(const Fq2x52 &a)
+{
+    const Fq52 p = (a.c0 + a.c1) * (a.c0 - a.c1);
+    const Fq52 q = a.c0 * a.c1;
+    return {p, q + q};
+}
+
+// ---------------------------------------------------------------------------
+// storage <-> compute: bits only (the stored value is already in the R' domain)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ Fq52 to52(const Fq &x)
+{
+    uint64_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) w[i] = uint64_t(x.v[2 * i]) | (uint64_t(x.v[2 * i + 1]) << 32);
+    Fq52 r;
+    r.l[0] = w[0] & f52::kMask;
+    r.l[1] = ((w[0] >> 52) | (w[1] << 12)) & f52::kMask;
+    r.l[2] = ((w[1] >> 40) | (w[2] << 24)) & f52::kMask;
+    r.l[3] = ((w[2] >> 28) | (w[3] << 36)) & f52::kMask;
+    r.l[4] = w[3] >> 16;
+    return r;
+}
+
+__device__ __forceinline__ Fq from52(const Fq52 &x)
+{
+    uint64_t w[4];
+    w[0] = x.l[0] | (x.l[1] << 52);
+    w[1] = (x.l[1] >> 12) | (x.l[2] << 40);
+    w[2] = (x.l[2] >> 24) | (x.l[3] << 28);
+    w[3] = (x.l[3] >> 36) | (x.l[4] << 16);
+    Fq r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        r.v[2 * i] = uint32_t(w[i]);
+        r.v[2 * i + 1] = uint32_t(w[i] >> 32);
+    }
+    return r;
+}
+
+__device__ __forceinline__ Fq52 to_compute(const Fq &x) { return to52(x); }
+__device__ __forceinline__ Fq2x52 to_compute(const Fq2 &x) { return {to52(x.c0), to52(x.c1)}; }
+__device__ __forceinline__ Fq to_storage(const Fq52 &x) { return from52(x); }
+__device__ __forceinline__ Fq2 to_storage(const Fq2x52 &x) { return {from52(x.c0), from52(x.c1)}; }
+
+template <class S>
+struct Compute;
+template <>
+struct Compute<Fq> {
+    using type = Fq52;
+};
+template <>
+struct Compute<Fq2> {
+    using type = Fq2x52;
+};
+
+// Montgomery domain changes: x 2^256 -> x 2^260 (times 2^264 mod p) and back
+// (times 2^256 mod p), each one R' product
+__device__ __forceinline__ Fq52 r256_to_r260(const Fq52 &x)
+{
+    return mul52(x, Fq52{{0xb0f2afaec667aull, 0xed9626b0fffbdull, 0x9e2a0fcad825aull,
+                          0xe357276f48b70ull, 0xd791464ef86ull}});
+}
+__device__ __forceinline__ Fq52 r260_to_r256(const Fq52 &x)
+{
+    return mul52(x, Fq52{{0xd438dc58f0d9dull, 0x28f5c70b3dd35ull, 0x879462c0a78ebull,
+                          0xdf2f666ea36f7ull, 0xe0a77c19a07ull}});
+}
+__device__ __forceinline__ Fq2x52 r256_to_r260(const Fq2x52 &x)
+{
+    return {r256_to_r260(x.c0), r256_to_r260(x.c1)};
+}
+__device__ __forceinline__ Fq2x52 r260_to_r256(const Fq2x52 &x)
+{
+    return {r260_to_r256(x.c0), r260_to_r256(x.c1)};
+}
+
+} // namespace nkr

@@ -4,8 +4,10 @@
 // product is compiled out of line (one body per kernel) to keep the hot loops
 // resident in the instruction cache.
 #define NKR_FIELD_MUL_OUTLINE 1
+#include <algorithm>
 #include <cstring>
 
+#include "field52.cuh"
 #include "msm.cuh"
 #include "scan.cuh"
 
@@ -99,6 +101,54 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
     });
 }
 
+// --------------------------------------------------------------------------
+// storage vs compute.  G1 arithmetic runs on the FP64 pipe (Fq52, R' = 2^260):
+// every G1 MSM buffer (bases, partials, buckets, reduction items) holds R'-domain
+// values in the 8 x 32-bit layout of Fq, converted at entry (bases) and exit
+// (result).  G2 arithmetic stays on the integer pipe (Fq2, R = 2^256): measured,
+// its FP64 form needs more than 255 registers and ran 30% slower.
+// --------------------------------------------------------------------------
+
+template <class F>
+struct MsmArith;
+template <>
+struct MsmArith<Fq> {
+    using type = Fq52;
+};
+template <>
+struct MsmArith<Fq2> {
+    using type = Fq2;
+};
+template <class F>
+using CF = typename MsmArith<F>::type;
+
+__device__ __forceinline__ Fq52 msm_in(const Fq &x) { return to52(x); }
+__device__ __forceinline__ Fq msm_out(const Fq52 &x) { return from52(x); }
+__device__ __forceinline__ Fq52 msm_enter(const Fq52 &x) { return r256_to_r260(x); }
+__device__ __forceinline__ Fq52 msm_leave(const Fq52 &x) { return r260_to_r256(x); }
+__device__ __forceinline__ Fq2 msm_in(const Fq2 &x) { return x; }
+__device__ __forceinline__ Fq2 msm_out(const Fq2 &x) { return x; }
+__device__ __forceinline__ Fq2 msm_enter(const Fq2 &x) { return x; }
+__device__ __forceinline__ Fq2 msm_leave(const Fq2 &x) { return x; }
+
+template <class F>
+__device__ __forceinline__ Xyzz<CF<F>> ldx(const Xyzz<F> &s)
+{
+    return {msm_in(s.x), msm_in(s.y), msm_in(s.zz), msm_in(s.zzz)};
+}
+
+template <class C>
+__device__ __forceinline__ auto stx(const Xyzz<C> &c) -> Xyzz<decltype(msm_out(c.x))>
+{
+    return {msm_out(c.x), msm_out(c.y), msm_out(c.zz), msm_out(c.zzz)};
+}
+
+template <class F>
+__device__ __forceinline__ Affine<CF<F>> lda(const Affine<F> &s)
+{
+    return {msm_in(s.x), msm_in(s.y)};
+}
+
 // first index in a[0, n) with a[idx] > x (a nondecreasing)
 __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t *a, uint32_t n, uint32_t x)
 {
@@ -140,12 +190,19 @@ __device__ __forceinline__ Pieces bucket_pieces(const uint32_t *offsets, uint32_
 
 // Groups of k2 pieces a bucket still has at a fix-up level whose inputs are
 // spaced `stride` pieces apart (zero once the bucket is complete).
+constexpr unsigned kFixupBlocks = 148 * 8; // grid cap of a fix-up level
+
+// Buckets of at most kSmallPieces pieces are summed where they are consumed
+// (k_reduce_first); only larger ones go through the fix-up levels.
+constexpr uint32_t kSmallPieces = 16;
+
 struct LoadLeaders {
     const uint32_t *offsets;
     uint32_t k1, stride, k2;
     __device__ __forceinline__ uint32_t operator()(uint64_t i) const
     {
         const Pieces pc = bucket_pieces(offsets, uint32_t(i), k1);
+        if (pc.count <= kSmallPieces) return 0u;
         const uint32_t live = (pc.count + stride - 1) / stride;
         return live > 1 ? (live + k2 - 1) / k2 : 0u;
     }
@@ -172,17 +229,18 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
     uint32_t b = upper_bound_u32(offsets, nb + 1, beg) - 1; // offsets[b] <= beg < offsets[b + 1]
     uint32_t bstart = offsets[b], bend = offsets[b + 1];
     bool first = true;
-    Xyzz<F> acc = Xyzz<F>::inf();
+    using C = CF<F>;
+    Xyzz<C> acc = Xyzz<C>::inf();
     // one flat loop with the same trip count in every lane keeps the additions
     // converged; the flush at a bucket boundary is a short divergent branch
     for (uint32_t j = beg; j < end; ++j) {
         if (j == bend) {
             if (bstart >= beg)
-                buckets[b] = acc; // the bucket started and ended inside the segment
+                buckets[b] = stx(acc); // the bucket started and ended inside the segment
             else
-                partials[2ull * t] = acc; // first run, bucket began in an earlier segment
+                partials[2ull * t] = stx(acc); // first run, bucket began in an earlier segment
             first = false;
-            acc = Xyzz<F>::inf();
+            acc = Xyzz<C>::inf();
             // next nonempty bucket: usually adjacent, else search
             ++b;
             int steps = 0;
@@ -195,19 +253,45 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
             bend = offsets[b + 1];
         }
         const uint32_t e = entries[j];
-        Affine<F> p = pts[e & 0x7fffffffu];
+        Affine<C> p = lda(pts[e & 0x7fffffffu]);
         if (e >> 31) p = affine_neg(p);
         acc = xyzz_add_affine(acc, p);
     }
     if (bstart >= beg && bend <= end)
-        buckets[b] = acc;
+        buckets[b] = stx(acc);
     else
-        partials[2ull * t + (first ? 0 : 1)] = acc;
+        partials[2ull * t + (first ? 0 : 1)] = stx(acc);
 }
 
-// One thread per group of k2 pieces (spaced `stride` pieces apart) of one
-// bucket; the group's sum goes back into the group's first piece slot, or into
-// the bucket when it was the bucket's last group.
+// One group of k2 pieces (spaced `stride` pieces apart) of one bucket; the
+// group's sum goes back into the group's first piece slot, or into the bucket
+// when it was the bucket's last group.
+template <class F>
+__device__ __forceinline__ void acc_up_group(const uint32_t *__restrict__ offsets,
+                                             const uint32_t *__restrict__ lead_off, uint32_t nb,
+                                             uint32_t k1, Xyzz<F> *__restrict__ partials,
+                                             Xyzz<F> *__restrict__ buckets, uint32_t stride,
+                                             uint32_t k2, uint32_t q)
+{
+    const uint32_t b = upper_bound_u32(lead_off, nb + 1, q) - 1;
+    const uint32_t j = q - lead_off[b];
+    const Pieces pc = bucket_pieces(offsets, b, k1);
+    const uint32_t off_b = offsets[b];
+    const uint32_t live = (pc.count + stride - 1) / stride;
+    const uint64_t r = uint64_t(j) * k2 * stride;
+    Xyzz<CF<F>> acc = Xyzz<CF<F>>::inf();
+    for (uint32_t m = 0; m < k2; ++m) {
+        const uint64_t idx = r + uint64_t(m) * stride;
+        if (idx >= pc.count) break;
+        acc = xyzz_add(acc, ldx(partials[pc.slot(off_b, k1, uint32_t(idx))]));
+    }
+    if (live <= k2)
+        buckets[b] = stx(acc);
+    else
+        partials[pc.slot(off_b, k1, uint32_t(r))] = stx(acc);
+}
+
+// Fix-up level: a grid-stride loop over the level's groups (often none).
 template <class F>
 __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ offsets,
                                                  const uint32_t *__restrict__ lead_off, uint32_t nb,
@@ -216,50 +300,63 @@ __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ off
                                                  uint32_t k2)
 {
     const uint32_t total = lead_off[nb];
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= total) return;
-    const uint32_t b = upper_bound_u32(lead_off, nb + 1, q) - 1;
-    const uint32_t j = q - lead_off[b];
-    const Pieces pc = bucket_pieces(offsets, b, k1);
-    const uint32_t off_b = offsets[b];
-    const uint32_t live = (pc.count + stride - 1) / stride;
-    const uint64_t r = uint64_t(j) * k2 * stride;
-    Xyzz<F> acc = Xyzz<F>::inf();
-    for (uint32_t m = 0; m < k2; ++m) {
-        const uint64_t idx = r + uint64_t(m) * stride;
-        if (idx >= pc.count) break;
-        acc = xyzz_add(acc, partials[pc.slot(off_b, k1, uint32_t(idx))]);
-    }
-    if (live <= k2)
-        buckets[b] = acc;
-    else
-        partials[pc.slot(off_b, k1, uint32_t(r))] = acc;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
+        acc_up_group(offsets, lead_off, nb, k1, partials, buckets, stride, k2, q);
 }
 
 // --------------------------------------------------------------------------
 // bucket reduction: sum_b b * S_b per set, then + sum_b S_b
 // --------------------------------------------------------------------------
 
-// Work-efficient first level for large bucket sets: a thread takes L
-// consecutive buckets and forms T = sum_i i S_i and R = sum_i S_i by running
-// sums (2 additions per bucket), emitting one (A = T, R) item per L buckets
-// with unit L for the block levels that follow.
+// buckets per thread of the first reduction level (log2): about 2^16 threads
+// (short dependent chains, enough warps), at most 16 buckets each
+__host__ __device__ constexpr int first_level_log2(uint32_t m)
+{
+    int lg = 0;
+    while ((uint64_t(1) << (lg + 1)) <= m) ++lg;
+    return lg <= 16 ? 0 : lg - 16 > 4 ? 4 : lg - 16;
+}
+
+// run += S_b for bucket b: S_b is empty, written whole by the level-1 kernel
+// (one piece) or by the fix-up levels (more than kSmallPieces pieces), or else
+// its few pieces are added straight from the partial slots.
 template <class F>
-__global__ void __launch_bounds__(128) k_reduce_chunk(const Xyzz<F> *__restrict__ r_in,
-                                                       uint64_t items, uint32_t L,
+__device__ __forceinline__ Xyzz<CF<F>> add_bucket_sum(Xyzz<CF<F>> run,
+                                                      const uint32_t *__restrict__ offsets,
+                                                      const Xyzz<F> *__restrict__ partials,
+                                                      const Xyzz<F> *__restrict__ buckets, uint32_t b,
+                                                      uint32_t k1)
+{
+    const uint32_t lo = offsets[b], hi = offsets[b + 1];
+    if (hi == lo) return run;
+    const Pieces pc{lo / k1, (hi - 1) / k1 - lo / k1 + 1};
+    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldx(buckets[b]));
+    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldx(partials[pc.slot(lo, k1, k)]));
+    return run;
+}
+
+// Work-efficient first reduction level: a thread takes L consecutive buckets
+// and forms T = sum_i i S_i and R = sum_i S_i by running sums (2 additions per
+// bucket), emitting one (A = T, R) item per L buckets with unit L for the block
+// levels that follow.  Bucket sums of few pieces are finished here.
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict__ offsets,
+                                                       const Xyzz<F> *__restrict__ partials,
+                                                       const Xyzz<F> *__restrict__ buckets,
+                                                       uint64_t items, uint32_t L, uint32_t k1,
                                                        Xyzz<F> *__restrict__ a_out,
                                                        Xyzz<F> *__restrict__ r_out)
 {
     const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t * L >= items) return;
     const uint64_t base = t * L;
-    Xyzz<F> run = Xyzz<F>::inf(), tri = Xyzz<F>::inf();
+    Xyzz<CF<F>> run = Xyzz<CF<F>>::inf(), tri = Xyzz<CF<F>>::inf();
     for (int i = int(L) - 1; i >= 0; --i) {
-        run = xyzz_add(run, r_in[base + i]);
+        run = add_bucket_sum(run, offsets, partials, buckets, uint32_t(base + i), k1);
         if (i > 0) tri = xyzz_add(tri, run);
     }
-    a_out[t] = tri;
-    r_out[t] = run;
+    a_out[t] = stx(tri);
+    r_out[t] = stx(run);
 }
 
 // One level of the weighted sum: items carry (A_c, R_c) with
@@ -277,9 +374,10 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
                                                       Xyzz<F> *__restrict__ a_out,
                                                       Xyzz<F> *__restrict__ r_out)
 {
+    using C = CF<F>;
     extern __shared__ uint8_t smem_raw[];
-    Xyzz<F> *buf0 = reinterpret_cast<Xyzz<F> *>(smem_raw);
-    Xyzz<F> *buf1 = buf0 + BS;
+    Xyzz<C> *buf0 = reinterpret_cast<Xyzz<C> *>(smem_raw);
+    Xyzz<C> *buf1 = buf0 + BS;
     const uint32_t blocks_per_set = (m + BS - 1) / BS;
     const uint32_t set = blockIdx.x / blocks_per_set;
     const uint32_t blk = blockIdx.x % blocks_per_set;
@@ -287,23 +385,23 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     const uint64_t idx = uint64_t(blk) * BS + i;
     const bool live = idx < m;
     const uint64_t g = uint64_t(set) * m + idx;
-    Xyzz<F> v = live ? r_in[g] : Xyzz<F>::inf();
+    Xyzz<C> v = live ? ldx(r_in[g]) : Xyzz<C>::inf();
     buf0[i] = v;
     __syncthreads();
-    Xyzz<F> *cur = buf0, *nxt = buf1;
+    Xyzz<C> *cur = buf0, *nxt = buf1;
     for (int d = 1; d < BS; d <<= 1) {
         if (i + d < BS) v = xyzz_add(v, cur[i + d]);
         nxt[i] = v;
         __syncthreads();
-        Xyzz<F> *t = cur;
+        Xyzz<C> *t = cur;
         cur = nxt;
         nxt = t;
     }
     // v = Suf_i.  R' = Suf_0; weighted part = sum_{i >= 1} Suf_i; A part = sum A_i
-    const Xyzz<F> total = cur[0];
+    const Xyzz<C> total = cur[0];
     __syncthreads();
-    buf0[i] = i >= 1 ? v : Xyzz<F>::inf();
-    buf1[i] = (a_in && live) ? a_in[g] : Xyzz<F>::inf();
+    buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
+    buf1[i] = (a_in && live) ? ldx(a_in[g]) : Xyzz<C>::inf();
     __syncthreads();
     for (int s = BS / 2; s > 0; s >>= 1) {
         if (i < s) {
@@ -313,43 +411,57 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
         __syncthreads();
     }
     if (i == 0) {
-        Xyzz<F> w = buf0[0];
+        Xyzz<C> w = buf0[0];
         for (int d = 0; d < log2_unit; ++d) w = xyzz_dbl(w);
         const uint32_t o = set * blocks_per_set + blk;
-        a_out[o] = xyzz_add(w, buf1[0]);
-        r_out[o] = total;
+        a_out[o] = stx(xyzz_add(w, buf1[0]));
+        r_out[o] = stx(total);
     }
 }
 
 // XYZZ -> libff Jacobian layout without inversion: with Z = ZZ ZZZ,
-// X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point.
+// X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point; the
+// coordinates leave the R' domain here (back to the library's R = 2^256).
 template <class F>
-__device__ __forceinline__ void store_jacobian(const Xyzz<F> &p, F *out)
+__device__ __forceinline__ void store_jacobian(const Xyzz<CF<F>> &p, F *out)
 {
+    using C = CF<F>;
     if (p.is_inf()) {
         out[0] = F::zero();
         out[1] = F::one();
         out[2] = F::zero();
         return;
     }
-    const F zzz2 = sqr(p.zzz);
-    const F zz2 = sqr(p.zz);
-    out[0] = p.x * (p.zz * zzz2);
-    out[1] = p.y * (zz2 * p.zz * zzz2);
-    out[2] = p.zz * p.zzz;
+    const C zzz2 = sqr(p.zzz);
+    const C zz2 = sqr(p.zz);
+    out[0] = msm_out(msm_leave(p.x * (p.zz * zzz2)));
+    out[1] = msm_out(msm_leave(p.y * (zz2 * p.zz * zzz2)));
+    out[2] = msm_out(msm_leave(p.zz * p.zzz));
 }
 
 template <class F>
 __global__ void k_finalize(const Xyzz<F> *a, const Xyzz<F> *r, int sets, int c, F *out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Xyzz<F> acc = Xyzz<F>::inf();
+    using C = CF<F>;
+    Xyzz<C> acc = Xyzz<C>::inf();
     for (int k = sets - 1; k >= 0; --k) {
         if (k != sets - 1)
             for (int d = 0; d < c; ++d) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, a ? xyzz_add(a[k], r[k]) : r[k]);
+        acc = xyzz_add(acc, a ? xyzz_add(ldx(a[k]), ldx(r[k])) : ldx(r[k]));
     }
-    store_jacobian(acc, out);
+    store_jacobian<F>(acc, out);
+}
+
+// Resident bases enter the R' domain once they are final (x 2^4 mod p per
+// coordinate; the infinity encoding (0, one) maps to (0, one'))
+template <class F>
+__global__ void k_bases_to_r260(Affine<F> *__restrict__ pts, uint64_t n)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Affine<CF<F>> a = lda(pts[i]);
+    pts[i] = {msm_out(msm_enter(a.x)), msm_out(msm_enter(a.y))};
 }
 
 // --------------------------------------------------------------------------
@@ -479,7 +591,7 @@ template <class F>
 int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
     const MsmShape &sh = bs.shape;
-    NKR_CUDA(cudaMemsetAsync(a.buckets.p, 0, uint64_t(sh.nb) * sizeof(Xyzz<F>), st));
+    // no bucket clearing: a bucket is read only after the kernel that wrote it
     const uint64_t segs = sh.segments_max();
     const uint32_t *offsets = s.offsets.as<uint32_t>();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[0], st));
@@ -495,7 +607,8 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
         NKR_TRY(scan_exclusive(LoadLeaders{offsets, uint32_t(sh.k1), uint32_t(stride), uint32_t(k2)},
                                sh.nb, a.lead_off.as<uint32_t>(), a.scan_tmp.as<uint32_t>(), st));
         const uint64_t bound = 2 * segs / (stride * k2) + sh.nb + 1;
-        k_acc_up<F><<<blocks_for(bound, 128), 128, 0, st>>>(offsets, a.lead_off.as<uint32_t>(), sh.nb,
+        const unsigned grid = std::min<unsigned>(blocks_for(bound, 128), kFixupBlocks);
+        k_acc_up<F><<<grid, 128, 0, st>>>(offsets, a.lead_off.as<uint32_t>(), sh.nb,
                                                             uint32_t(sh.k1), a.partials.as<Xyzz<F>>(),
                                                             a.buckets.as<Xyzz<F>>(), uint32_t(stride),
                                                             uint32_t(k2));
@@ -504,29 +617,26 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     // bucket reduction levels
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     uint32_t m = sh.B;
-    const Xyzz<F> *a_in = nullptr;
-    const Xyzz<F> *r_in = a.buckets.as<Xyzz<F>>();
     Xyzz<F> *bufs_a[2] = {a.red_a.as<Xyzz<F>>(), a.red_a2.as<Xyzz<F>>()};
     Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
-    int flip = 0, log2_unit = 0;
     constexpr int BS = sizeof(F) == sizeof(Fq) ? 256 : 128; // G1: 256 buckets per block, G2: 128
     constexpr int kLog2BS = BS == 256 ? 8 : 7;
-    const size_t smem = 2 * BS * sizeof(Xyzz<F>);
+    const size_t smem = 2 * BS * sizeof(Xyzz<CF<F>>);
     NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
-    if (m >= (1u << 16)) {
-        // large sets: one work-efficient pass of 16 buckets per thread first
-        constexpr uint32_t L = 16;
-        const uint64_t items = uint64_t(sets) * m;
-        k_reduce_chunk<F><<<blocks_for(items / L, 128), 128, 0, st>>>(r_in, items, L, bufs_a[0],
-                                                                      bufs_r[0]);
-        NKR_CHECK_LAUNCH();
-        a_in = bufs_a[0];
-        r_in = bufs_r[0];
-        flip = 1;
-        m /= L;
-        log2_unit = 4;
-    }
+    // first level: bucket sums (few-piece buckets finished here), L buckets per thread
+    const int log2_l = first_level_log2(m);
+    const uint32_t L = 1u << log2_l;
+    const uint64_t items = uint64_t(sets) * m;
+    k_reduce_first<F><<<blocks_for(items / L, 128), 128, 0, st>>>(
+        offsets, a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), items, L, uint32_t(sh.k1), bufs_a[0],
+        bufs_r[0]);
+    NKR_CHECK_LAUNCH();
+    const Xyzz<F> *a_in = bufs_a[0];
+    const Xyzz<F> *r_in = bufs_r[0];
+    int flip = 1;
+    m /= L;
+    int log2_unit = log2_l;
     while (m > 1) {
         const uint32_t per_set = (m + BS - 1) / BS;
         k_reduce_block<F, BS><<<sets * per_set, BS, smem, st>>>(a_in, r_in, m, log2_unit, bufs_a[flip],
@@ -547,7 +657,8 @@ template <class F>
 int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
 {
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
-    const uint64_t red = uint64_t(sets) * (sh.B / 8 + 1);
+    // first reduction level output: one item per L buckets (L as in acc_run_t)
+    const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B)) + 1;
     NKR_TRY(a.partials.alloc(2 * std::max<uint64_t>(sh.segments_max(), 1) * sizeof(Xyzz<F>),
                              "msm partial sums"));
     NKR_TRY(a.buckets.alloc(uint64_t(sh.nb) * sizeof(Xyzz<F>), "msm buckets"));
@@ -643,6 +754,11 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
         NKR_CUDA(cudaStreamSynchronize(st));
     }
     if (folded) NKR_TRY(group == 1 ? build_windows_t<Fq>(b, st) : build_windows_t<Fq2>(b, st));
+    const uint64_t total = n * copies;
+    if (group == 1) { // G2 computes in the library's own domain
+        k_bases_to_r260<Fq><<<blocks_for(total, 128), 128, 0, st>>>(b.pts.as<G1Affine>(), total);
+        NKR_CHECK_LAUNCH();
+    }
     NKR_CUDA(cudaStreamSynchronize(st));
     return NKR_B200_OK;
 }

@@ -1,6 +1,7 @@
 // Elementwise field / group kernels behind nkr_b200_field_op and
 // nkr_b200_group_op (used by the parity tests against the oracle), and the
 // Montgomery-product throughput microbenchmark that gives the integer roofline.
+#include "field52.cuh"
 #include "curve.cuh"
 #include "ops.cuh"
 
@@ -49,6 +50,27 @@ __global__ void k_fq2_op(int op, const Fq2 *a, const Fq2 *b, Fq2 *out, uint64_t 
     default: r = x;
     }
     out[i] = r;
+}
+
+// The same ops in the FP64-limb arithmetic (R' = 2^260): inputs and outputs in
+// the library's R = 2^256 Montgomery form, converted at both ends.
+template <class S>
+__global__ void k_field52_op(int op, const S *a, const S *b, S *out, uint64_t n)
+{
+    using C = typename Compute<S>::type;
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const C x = r256_to_r260(to_compute(a[i]));
+    const C y = r256_to_r260(to_compute(b ? b[i] : a[i]));
+    C r;
+    switch (op) {
+    case 0: r = x * y; break;
+    case 1: r = x + y; break;
+    case 2: r = x - y; break;
+    case 3: r = sqr(x); break;
+    default: r = neg(x);
+    }
+    out[i] = to_storage(r260_to_r256(r));
 }
 
 // points in libff layout (X, Y, Z) with Z in {0, 1}
@@ -125,6 +147,32 @@ __global__ void k_check_wide(const Fp<P> *a, const Fp<P> *b, uint32_t *bad, int 
     if (i < n && mont_mul_cc(a[i], b[i]) != a[i] * b[i]) atomicAdd(bad, 1u);
 }
 
+// The 52-bit-limb product (R = 2^260) times 2^4 equals the library product (R = 2^256).
+__global__ void k_check_52(const Fq *a, const Fq *b, uint32_t *bad, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fq r = from52(mul52(to52(a[i]), to52(b[i])));
+    for (int k = 0; k < 4; ++k) r = dbl(r);
+    if (r != a[i] * b[i]) atomicAdd(bad, 1u);
+}
+
+__global__ void __launch_bounds__(256) k_bench_mul52(const Fq *seed, Fq *sink)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    Fq52 a = to52(seed[i & 255]), b = to52(seed[(i + 1) & 255]), c = to52(seed[(i + 2) & 255]),
+         d = to52(seed[(i + 3) & 255]);
+    const Fq52 m = to52(seed[(i + 7) & 255]);
+    for (int k = 0; k < kBenchIters; ++k) {
+        a = mul52(a, m);
+        b = mul52(b, m);
+        c = mul52(c, m);
+        d = mul52(d, m);
+    }
+    const Fq r = from52(a) + from52(b) + from52(c) + from52(d);
+    if (r.v[0] == 0x12345678u) sink[i] = r;
+}
+
 } // namespace
 
 int field_op_device(int field, int op, const void *a, const void *b, void *out, uint64_t n,
@@ -143,6 +191,14 @@ int field_op_device(int field, int op, const void *a, const void *b, void *out, 
         NKR_REQUIRE(op <= 4, "Fq2 supports ops 0..4");
         k_fq2_op<<<g, 128, 0, st>>>(op, static_cast<const Fq2 *>(a), static_cast<const Fq2 *>(b),
                                     static_cast<Fq2 *>(out), n);
+    } else if (field == 3 || field == 4) {
+        NKR_REQUIRE(op <= 4, "52-bit-limb field ops are 0..3 and 4 (negation)");
+        if (field == 3)
+            k_field52_op<Fq><<<g, 128, 0, st>>>(op, static_cast<const Fq *>(a), static_cast<const Fq *>(b),
+                                                static_cast<Fq *>(out), n);
+        else
+            k_field52_op<Fq2><<<g, 128, 0, st>>>(op, static_cast<const Fq2 *>(a),
+                                                 static_cast<const Fq2 *>(b), static_cast<Fq2 *>(out), n);
     } else {
         NKR_REQUIRE(false, "field %d unknown", field);
     }
@@ -188,18 +244,21 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
     float best = 1e30f;
     const int variant = field >> 8;
     field &= 0xff;
-    if (variant == 1) {
+    if (variant == 1 || variant == 3) {
         // the alternative product must agree with operator* before it is timed
         DevBuf bad;
         NKR_TRY(bad.alloc(4, "bench check"));
         NKR_CUDA(cudaMemsetAsync(bad.p, 0, 4, st));
-        k_check_wide<FqParams><<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1, bad.as<uint32_t>(),
-                                                   255);
+        if (variant == 1)
+            k_check_wide<FqParams><<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1,
+                                                       bad.as<uint32_t>(), 255);
+        else
+            k_check_52<<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1, bad.as<uint32_t>(), 255);
         NKR_CHECK_LAUNCH();
         uint32_t nbad = 0;
         NKR_CUDA(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, st));
         NKR_CUDA(cudaStreamSynchronize(st));
-        NKR_REQUIRE(nbad == 0, "carry-chain product disagrees on %u inputs", nbad);
+        NKR_REQUIRE(nbad == 0, "alternative product (variant %d) disagrees on %u inputs", variant, nbad);
     }
     for (int rep = 0; rep < 4; ++rep) {
         NKR_CUDA(cudaEventRecord(e0, st));
@@ -209,6 +268,8 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
             k_bench_mul<FqParams, 0><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         else if (variant == 1)
             k_bench_mul<FqParams, 1><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+        else if (variant == 3)
+            k_bench_mul52<<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         else
             k_bench_mul<FqParams, 2><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         NKR_CHECK_LAUNCH();

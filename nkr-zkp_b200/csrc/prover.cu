@@ -154,6 +154,8 @@ int slot_add(nkr_b200_key *key)
     NKR_CUDA(cudaSetDevice(key->ctx->device));
     auto slot = std::make_unique<ProveSlot>();
     ProveSlot *sl = slot.get();
+    // (a higher priority for the main stream was measured slower: the H chain
+    // finishes early but the H MSM then crowds out the witness MSMs)
     for (int k = 0; k < kNumMsm; ++k) {
         NKR_CUDA(cudaStreamCreateWithFlags(&sl->st[k], cudaStreamNonBlocking));
         NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_done[k], cudaEventDisableTiming));

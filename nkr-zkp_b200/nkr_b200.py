@@ -283,7 +283,7 @@ class Context:
         return out
 
     def field_op(self, field, op, a, b=None):
-        w = 8 if field == 2 else 4
+        w = 8 if field in (2, 4) else 4
         a = np.ascontiguousarray(a, np.uint64).reshape(-1, w)
         bb = None if b is None else np.ascontiguousarray(b, np.uint64).reshape(-1, w)
         out = np.zeros_like(a)

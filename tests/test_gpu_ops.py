@@ -40,6 +40,33 @@ def test_field_ops_exact(ctx, rng, field, mod):
     assert np.array_equal(ctx.field_op(field, 6, m), canon)
 
 
+def test_fp64_limb_arithmetic_matches_integer_arithmetic(ctx, rng):
+    """The MSM's FP64-limb Fq (five 52-bit limbs, R = 2^260; fields 3 and 4) gives
+    exactly the integer library's results (fields 1 and 2) on edge and random values."""
+    a_int = _edge_and_random(O.P, rng, n=2000)
+    b_int = list(reversed(a_int))
+    a = np.stack([O.fq_mont(x) for x in a_int])
+    b = np.stack([O.fq_mont(x) for x in b_int])
+    for op in range(4):
+        assert np.array_equal(ctx.field_op(3, op, a, b), ctx.field_op(1, op, a, b)), f"op {op}"
+    neg = ctx.field_op(3, 4, a)
+    assert all(O.fq_int(neg[i]) == (-x) % O.P for i, x in enumerate(a_int))
+    a2 = np.concatenate([a, b], axis=1)
+    b2 = np.concatenate([b[::-1], a[::-1]], axis=1)
+    P = O.P
+    for field, op in [(f, o) for o in range(4) for f in (2, 4)]:
+        got = ctx.field_op(field, op, a2, b2)
+        bad = []
+        for i in range(len(a_int)):
+            x0, x1, y0, y1 = a_int[i], b_int[i], b_int[::-1][i], a_int[::-1][i]
+            want = {0: ((x0 * y0 - x1 * y1) % P, (x0 * y1 + x1 * y0) % P),
+                    1: ((x0 + y0) % P, (x1 + y1) % P), 2: ((x0 - y0) % P, (x1 - y1) % P),
+                    3: ((x0 * x0 - x1 * x1) % P, 2 * x0 * x1 % P)}[op]
+            if (O.fq_int(got[i][:4]), O.fq_int(got[i][4:])) != want:
+                bad.append((i, hex(x0), hex(x1), hex(y0), hex(y1)))
+        assert not bad, f"field {field} op {op}: {len(bad)} wrong, first {bad[:3]}"
+
+
 def test_fq2_ops_exact(ctx, rng):
     n = 64
     ai = [(int.from_bytes(rng.bytes(32), "little") % O.P, int.from_bytes(rng.bytes(32), "little") % O.P)
