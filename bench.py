@@ -139,9 +139,11 @@ def cpu_baseline_reference(sample=REF_SAMPLE):
         ref = O.Ref()
         ref.cpu_setup(r1, os.path.join(d, "pk"), os.path.join(d, "vk"))
         h = ref.prover(r1, os.path.join(d, "pk"))
+        reps = 2  # about 12 s of single-threaded CPU work
         t0 = time.perf_counter()
-        ref.prover_prove(h, r1.witness)
-        dt = time.perf_counter() - t0
+        for _ in range(reps):
+            ref.prover_prove(h, r1.witness)
+        dt = (time.perf_counter() - t0) / reps
         ref.prover_close(h)
         kind_s = "reference"
     else:
@@ -166,8 +168,8 @@ def cpu_baseline_reference(sample=REF_SAMPLE):
         kind_s = "port"
     scale = (1 << 20) / r1.rows
     return dt * 1e3 * scale, kind_s, (f"{kind} count={param} density=sparse ({r1.rows} constraints), "
-                                      f"one single-threaded prove {dt:.2f} s, scaled x{scale:.0f} "
-                                      "(linear in constraints) to 2^20")
+                                      f"single-threaded prove {dt:.2f} s (mean of the proves run), "
+                                      f"scaled x{scale:.0f} (linear in constraints) to 2^20")
 
 
 def _ref_worker(args):
@@ -217,7 +219,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(ms_per_proof, 3), "unit": "ms",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (u32 limbs, exact)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)",
         "data": "synthetic (seeded circuit, witness and toxic waste)",
         "config": {"workload": "groth16-prove poseidon count=2048 density=sparse (2^20 constraints)",
                    "sample": f"{kind} count={param} sparse ({r1.rows} constraints) per process, "
@@ -316,7 +318,12 @@ def run_b200(args):
 
     # ---- roofline of the dominant kernel (MSM bucket accumulation) ---------------
     peaks = _measured_peaks()
-    muls_peak, _ = ctx.bench_mul(1)
+    # the denominator is the fastest Fq product this GPU sustains in registers: the
+    # integer-pipe CIOS (variant 0) and the FP64-pipe 52-bit-limb product (variant 3,
+    # the one the G1 accumulation runs on); the larger one is the roof
+    peak_int, _ = ctx.bench_mul(1)
+    peak_fp64, _ = ctx.bench_mul(1 | (3 << 8))
+    muls_peak = max(peak_int, peak_fp64)
     mb = nk.MsmBases(ctx, 1, be._keep["a_query"]) if hasattr(be, "_keep") and be._keep else None
     roof = None
     if mb is not None:
@@ -338,8 +345,10 @@ def run_b200(args):
         roof = {"bound": "int", "kernel": "k_acc_l1<Fq> (G1 bucket accumulation)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),
                 "unit": "G Fq-mul/s", "frac": round(achieved / muls_peak, 3),
-                "peak_source": "measured: nkr_b200_bench_mul register-resident Montgomery products "
-                               "(MEASURED_PEAKS.json has no integer peak)",
+                "peak_source": "measured: nkr_b200_bench_mul register-resident Fq Montgomery "
+                               "products, best formulation (MEASURED_PEAKS.json has no integer peak)",
+                "peak_by_pipe": {"int_cios": round(peak_int / 1e9, 2),
+                                 "fp64_52bit": round(peak_fp64 / 1e9, 2)},
                 "units_per_launch": {"entries": st["entries"], "fq_muls": muls,
                                      "window_bits": st["window_bits"], "windows": st["windows"],
                                      "buckets": st["buckets"]},
@@ -369,7 +378,7 @@ def run_b200(args):
         "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (u32 limbs, exact)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)",
         "data": "synthetic (seeded circuit, witness and toxic waste)",
         "config": {"workload": f"groth16-prove {kind} count={param} density="
                                f"{['full', 'hybrid', 'sparse'][dens]} ({r1.rows} constraints, "
@@ -474,7 +483,7 @@ def run_batch(args):
     line = {
         "metric": "batched Groth16 proofs/s, 64 uneven proofs (bit-exact)", "value": round(bat_pps, 2),
         "unit": "proofs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "higher_is_better": True, "dtype": "bn254 (u32 limbs, exact)",
+        "higher_is_better": True, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)",
         "data": "synthetic (seeded circuits, witnesses and toxic waste)",
         "config": {"workload": "64 proofs: matmul s in [16, 64] or poseidon count 2^6..2^11, "
                                "hybrid density, seed 4", "domains": dict(sorted(hist.items())),
@@ -623,7 +632,7 @@ def run_serve(args):
     line = {
         "metric": "served Groth16 proofs/s and latency, Poisson stream over 6 resident keys",
         "value": round(n_req / srv_wall, 2), "unit": "proofs/s", "n_gpus": 1,
-        "higher_is_better": True, "dtype": "bn254 (u32 limbs, exact)", "bit_exact": ok,
+        "higher_is_better": True, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)", "bit_exact": ok,
         "data": "synthetic (seeded circuits, witnesses, toxic waste and arrivals)",
         "config": {"workload": "keys " + ", ".join(f"{k} {p}" for k, p, _ in keys),
                    "requests": n_req, "offered_load": args.serve_load,
@@ -644,6 +653,189 @@ def run_serve(args):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# standalone kernels: NTT, G1 / G2 MSM at the operator sizes
+# ---------------------------------------------------------------------------
+
+FR_MOD = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+_FR_LIMBS = [(FR_MOD >> (64 * i)) & (2**64 - 1) for i in range(4)]
+
+
+def _uniform_fr(n, rng):
+    """n uniform Fr elements as 4 x u64 limbs (read as Montgomery representations):
+    254-bit candidates, values >= r rejected."""
+    import numpy as np
+    out = np.empty((n, 4), np.uint64)
+    filled = 0
+    while filled < n:
+        k = n - filled
+        cand = rng.integers(0, 2**64, size=(k, 4), dtype=np.uint64)
+        cand[:, 3] &= np.uint64((1 << 62) - 1)
+        less = np.zeros(k, bool)
+        equal = np.ones(k, bool)
+        for i in range(3, -1, -1):
+            less |= equal & (cand[:, i] < np.uint64(_FR_LIMBS[i]))
+            equal &= cand[:, i] == np.uint64(_FR_LIMBS[i])
+        good = cand[less]
+        out[filled:filled + len(good)] = good
+        filled += len(good)
+    return out
+
+
+def _sparse_witness_scalars(n, rng):
+    """The sparse-witness mix: 10% uniform Fr, 30% zero, 60% drawn uniformly from
+    {zero, one, a small value < 2^16}, shuffled (Montgomery limbs)."""
+    import numpy as np
+    r_mont = pow(2, 256, FR_MOD)
+    small_tab = np.array([[(v * r_mont % FR_MOD >> (64 * i)) & (2**64 - 1) for i in range(4)]
+                          for v in range(1 << 16)], dtype=np.uint64)
+    out = np.zeros((n, 4), np.uint64)
+    n_uni, n_zero = n // 10, (3 * n) // 10
+    out[:n_uni] = _uniform_fr(n_uni, rng)
+    rest = n - n_uni - n_zero
+    cat = rng.integers(0, 3, rest)
+    vals = np.where(cat == 0, 0, np.where(cat == 1, 1, rng.integers(0, 1 << 16, rest)))
+    out[n_uni + n_zero:] = small_tab[vals]
+    return out[rng.permutation(n)]
+
+
+FQ_MOD = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+# affine generators of G1 = (1, 2) and of the G2 subgroup (x = x0 + x1 u, y = y0 + y1 u)
+G2_GEN = (10857046999023057135944570762232829481370756359578518086990519993285655852781,
+          11559732032986387107991004021392285783925812861821192530917403151452391805634,
+          8495653923123431417604973247489272438418190587263600148770280649306958101930,
+          4082367875863433681332203403145435568316851327593401208105741076214120093531)
+
+
+def _generator_jac(group):
+    """The group's generator in the libff Jacobian layout (Montgomery Fq limbs, Z = 1)."""
+    import numpy as np
+    coords = (1, 2, 1) if group == 1 else G2_GEN + (1, 0)
+    return np.array([(v * pow(2, 256, FQ_MOD) % FQ_MOD >> (64 * i)) & (2**64 - 1)
+                     for v in coords for i in range(4)], dtype=np.uint64)
+
+
+def _limb_ints(a):
+    return [int.from_bytes(row.tobytes(), "little") for row in a]
+
+
+def run_kernels(args):
+    """One JSON line: device time, work rate and a self-check of every standalone op."""
+    import numpy as np
+    import torch
+    import nkr_b200 as nk
+    ctx = nk.Context(0)
+    dev = "cuda:0"
+    rng = np.random.default_rng(11)
+    peaks = _measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    fr_peak, _ = ctx.bench_mul(0)
+    fq_peak = max(ctx.bench_mul(1)[0], ctx.bench_mul(1 | (3 << 8))[0])
+    clocks = ClockSampler(0)
+    clocks.start()
+    launches0 = nk.launch_count()
+    rows = []
+    r_inv = pow(2, -256, FR_MOD)
+
+    want = None if args.cases == "all" else set(args.cases.split(","))
+
+    def selected(name):
+        return want is None or name in want
+
+    # (i) NTT: FFT, iFFT, cosetFFT, icosetFFT at 2^16, 2^20, 2^24
+    for logn in (16, 20, 24):
+        if not selected(f"ntt.{logn}"):
+            continue
+        n = 1 << logn
+        host = _uniform_fr(n, rng)
+        x = torch.from_numpy(host.view(np.int64).reshape(-1)).to(dev)
+        work = torch.empty_like(x)
+        out = torch.empty_like(x)
+        back = torch.empty_like(x)
+        stream = torch.cuda.current_stream().cuda_stream  # the copies below run on it
+        for op, name, inv_op in ((0, "fft", 1), (1, "ifft", 0), (2, "coset_fft", 3), (3, "icoset_fft", 2)):
+            ts = []
+            for it in range(args.warmup + args.steps):
+                work.copy_(x)
+                ms = ctx.ntt_device(op, work.data_ptr(), out.data_ptr(), n, stream, timed=True)
+                if it >= args.warmup:
+                    ts.append(ms)
+            # round trip: the inverse op brings the input back bit for bit
+            work.copy_(out)
+            ctx.ntt_device(inv_op, work.data_ptr(), back.data_ptr(), n, stream)
+            torch.cuda.synchronize()
+            ok = bool(torch.equal(back, x))
+            ms = statistics.median(ts)
+            muls = (n // 2) * logn + (n if op != 0 else 0)  # butterflies + the coset / 1/N scale
+            byts = 2 * 32 * n * 2  # one transform read + write, one permuting read + write
+            rows.append({"op": f"ntt.{name}", "n": f"2^{logn}", "ms": round(ms, 4),
+                         "G_fr_mul_per_s": round(muls / ms / 1e6, 2),
+                         "frac_fr_mul_peak": round(muls / (ms * 1e-3) / fr_peak, 3),
+                         "GB_per_s": round(byts / ms / 1e6, 1),
+                         "frac_hbm": round(byts / (ms * 1e-3) / 1e9 / hbm_peak, 3),
+                         "check": "inverse round trip bit-exact" if ok else "ROUND TRIP FAILED"})
+        del x, work, out, back
+
+    # (ii)-(iv) MSM: bases k_i G from the library's scalar multiplication; the result
+    # must equal (sum_i s_i k_i) G computed by that independent double-and-add path
+    def msm_case(group, logn, mix):
+        n = 1 << logn
+        gen = _GEN[group]
+        w = 12 if group == 1 else 24
+        ks = _uniform_fr(n, rng)
+        bases = ctx.group_op(group, 2, np.tile(gen, (n, 1)), ks)
+        scal = _uniform_fr(n, rng) if mix == "uniform" else _sparse_witness_scalars(n, rng)
+        t_mont = sum(a * b for a, b in zip(_limb_ints(scal), _limb_ints(ks))) * r_inv % FR_MOD
+        want = ctx.group_op(group, 2, gen.reshape(1, w),
+                            np.array([[(t_mont >> (64 * i)) & (2**64 - 1) for i in range(4)]],
+                                     dtype=np.uint64))[0]
+        mb = nk.MsmBases(ctx, group, bases)
+        del bases
+        sd = torch.from_numpy(scal.view(np.int64).reshape(-1)).to(dev)
+        torch.cuda.synchronize()  # the MSM runs on the library's own stream
+        ts, accs = [], []
+        for it in range(args.warmup + args.steps):
+            got, ms = mb.run(None, scalars_ptr=sd.data_ptr())
+            if it >= args.warmup:
+                ts.append(ms)
+                accs.append(mb.stats()["acc_ms"])
+        st = mb.stats()
+        mb.free()
+        ok = bool(np.array_equal(got, want))
+        ms, acc_ms = statistics.median(ts), statistics.median(accs)
+        per_entry = 10 if group == 1 else 28  # mixed XYZZ add: 8M + 2S; Fq2 product = 3 Fq
+        muls = st["entries"] * per_entry
+        byts = n * (64 * group + 32)
+        return {"op": f"msm.g{group}.{mix}", "n": f"2^{logn}", "ms": round(ms, 4),
+                "window_bits": st["window_bits"], "windows": st["windows"], "entries": st["entries"],
+                "acc_ms": round(acc_ms, 4), "G_fq_mul_per_s_acc": round(muls / acc_ms / 1e6, 2),
+                "frac_fq_mul_peak_acc": round(muls / (acc_ms * 1e-3) / fq_peak, 3),
+                "G_fq_mul_per_s_whole": round(muls / ms / 1e6, 2),
+                "GB_per_s_algorithmic": round(byts / ms / 1e6, 1),
+                "check": "equals (sum s_i k_i) G" if ok else "MISMATCH"}
+
+    _GEN = {1: _generator_jac(1), 2: _generator_jac(2)}
+    for group, logn, mix in [(1, 16, "uniform"), (1, 16, "sparse"), (1, 20, "uniform"),
+                             (1, 20, "sparse"), (1, 22, "uniform"), (1, 22, "sparse"),
+                             (2, 18, "uniform"), (1, 18, "uniform")]:
+        # the 2^18 G1 case is the small profiling case (run only when named)
+        if (want is None and logn != 18) or (want is not None and f"msm.g{group}.{mix}.{logn}" in want):
+            rows.append(msm_case(group, logn, mix))
+    clk = clocks.stop()
+    line = {
+        "metric": "standalone NTT and MSM kernels: device ms per op (bit-exact self-checks)",
+        "value": None, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "dtype": "bn254 (exact modular)",
+        "data": "synthetic (seeded uniform Fr; bases k_i G with seeded k_i)",
+        "peaks": {"fr_mul_per_s": round(fr_peak / 1e9, 2), "fq_mul_per_s": round(fq_peak / 1e9, 2),
+                  "hbm_gbs": hbm_peak, "unit_mul": "G/s"},
+        "ops": rows, "all_checks_pass": all(not r["check"].isupper() for r in rows),
+        "gpu_launches": nk.launch_count() - launches0, "clocks": clk,
+    }
+    print(json.dumps(line))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -652,9 +844,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="poseidon2048", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="prove", choices=["prove", "batch", "serve"],
+    ap.add_argument("--mode", default="prove", choices=["prove", "batch", "serve", "kernels"],
                     help="prove: the 2^20 prove (default line); batch: 64 uneven proofs batched vs "
                          "plain; serve: Poisson requests over resident keys, server vs plain FIFO")
+    ap.add_argument("--cases", default="all",
+                    help="kernels mode: comma-separated subset, e.g. ntt.20,msm.g1.uniform.18 "
+                         "(ntt.{16,20,24}; msm.g1.{uniform,sparse}.{16,18,20,22}; msm.g2.uniform.18)")
     ap.add_argument("--serve-keys", type=int, default=6)
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.8)
@@ -666,6 +861,8 @@ def main():
         run_batch(args)
     elif args.mode == "serve":
         run_serve(args)
+    elif args.mode == "kernels":
+        run_kernels(args)
     else:
         run_b200(args)
 

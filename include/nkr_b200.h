@@ -135,9 +135,13 @@ int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses
  * No counterpart in the reference, which proves one request per process
  * (app/prove.cpp:70-88).  A scheduler thread admits waiting requests, oldest
  * first, onto free prove slots of their key (adding slots while free HBM allows,
- * up to max_slots_per_key per key and max_inflight in total) and replays each
- * slot's captured prove graph, so requests of different circuits overlap on the
- * GPU.  The witness memory of a request must stay valid until its wait returns.
+ * up to max_slots_per_key per key -- one for keys of 2^19 rows or more, which
+ * fill the GPU alone -- and max_inflight in total) and replays each slot's
+ * captured prove graph, so requests of different circuits overlap on the GPU.
+ * Slot streams take a priority by circuit size, so the GPU's block scheduler
+ * serves the smaller proofs in flight first (low median latency; the largest
+ * circuit's requests absorb the wait).  The witness memory of a request must
+ * stay valid until its wait returns.
  * A key added to a server is proved only through that server while it runs. */
 typedef struct nkr_b200_server nkr_b200_server;
 int nkr_b200_server_create(nkr_b200_ctx *ctx, int max_inflight, int max_slots_per_key,
@@ -159,6 +163,17 @@ void nkr_b200_server_destroy(nkr_b200_server *server);
  * Replaces NTTContext::{ntt,intt,coset_ntt,coset_intt} (ntt/ntt.cuh:110-185) and
  * libfqfft basic_radix2_domain.tcc:40-112. */
 int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n);
+
+/* The same five domain ops on device-resident vectors, as NTTContext runs them on
+ * its device arrays (ntt/ntt.cuh:110-185).  in and out are n Fr values each on the
+ * context's device and must not overlap; the result is written to out and in is
+ * overwritten (it is the transform's workspace).  stream is a cudaStream_t; NULL
+ * is CUDA's legacy default stream.  Work that produced `in` must be ordered before
+ * it on that stream.  The first call for a size builds that size's resident
+ * tables (allocation, synchronous); later calls only enqueue work unless device_ms
+ * is non-NULL, in which case the call waits and returns the ops' device time. */
+int nkr_b200_ntt_device(nkr_b200_ctx *ctx, int op, void *in, void *out, uint64_t n, void *stream,
+                        float *device_ms);
 
 /* The same five domain ops on DEVICE buffers, allocating no device memory.  No
  * counterpart in the reference: it serves callers that cannot allocate (their own

@@ -253,6 +253,70 @@ int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n)
     return NKR_B200_OK;
 }
 
+int nkr_b200_ntt_device(nkr_b200_ctx *ctx, int op, void *in, void *out, uint64_t n, void *stream,
+                        float *device_ms)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(in && out, "null data");
+    NKR_REQUIRE(op >= 0 && op <= 4, "ntt op %d unknown", op);
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT size %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)n);
+    const uint8_t *ib = static_cast<const uint8_t *>(in), *ob = static_cast<const uint8_t *>(out);
+    NKR_REQUIRE(ib + n * 32 <= ob || ob + n * 32 <= ib, "in and out overlap");
+    for (const void *p : {static_cast<const void *>(in), static_cast<const void *>(out)}) {
+        cudaPointerAttributes attr{};
+        const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+        if (e != cudaSuccess) cudaGetLastError();
+        NKR_REQUIRE(e == cudaSuccess && attr.type == cudaMemoryTypeDevice &&
+                        attr.device == ctx->device,
+                    "ntt_device buffers must be device memory of device %d", ctx->device);
+    }
+    const NttTables *T;
+    NKR_TRY(get_tables(ctx, logn, &T));
+    // NULL is CUDA's legacy default stream, so work the caller queued there (for
+    // instance the copy that filled `in`) is ordered before the transform
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (device_ms) {
+        NKR_CUDA(cudaEventCreate(&e0));
+        NKR_CUDA(cudaEventCreate(&e1));
+        NKR_CUDA(cudaEventRecord(e0, st));
+    }
+    const Fr *c = T->consts.as<Fr>();
+    Fr *pa = static_cast<Fr *>(in), *pb = static_cast<Fr *>(out);
+    switch (op) {
+    case 0:
+        NKR_TRY(ntt_dif(*T, pa, false, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, nullptr, st));
+        break;
+    case 1:
+        NKR_TRY(ntt_dif(*T, pa, true, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, c + kConstNinv, st));
+        break;
+    case 2:
+        NKR_TRY(ntt_dif(*T, pa, false, T->gpow.as<Fr>(), nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, nullptr, nullptr, st));
+        break;
+    case 3:
+        NKR_TRY(ntt_dif(*T, pa, true, nullptr, nullptr, nullptr, st));
+        NKR_TRY(ntt_bitrev_permute(pa, pb, n, T->t2.as<Fr>(), nullptr, st));
+        break;
+    case 4:
+        NKR_TRY(fr_scale_const(pa, n, c + kConstZinv, st));
+        NKR_CUDA(cudaMemcpyAsync(pb, pa, n * 32, cudaMemcpyDeviceToDevice, st));
+        break;
+    }
+    if (device_ms) {
+        NKR_CUDA(cudaEventRecord(e1, st));
+        NKR_CUDA(cudaEventSynchronize(e1));
+        NKR_CUDA(cudaEventElapsedTime(device_ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return NKR_B200_OK;
+}
+
 int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_t *row_ptr,
                   const uint32_t *col_idx, const void *values, const void *z, void *y)
 {

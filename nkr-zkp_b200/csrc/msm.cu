@@ -5,7 +5,9 @@
 // resident in the instruction cache.
 #define NKR_FIELD_MUL_OUTLINE 1
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "field52.cuh"
 #include "msm.cuh"
@@ -214,11 +216,11 @@ struct LoadLeaders {
 // a whole bucket is written to the bucket; the segment's first / last run, when
 // its bucket continues outside the segment, goes to partial slot 2t / 2t + 1.
 template <class F>
-__global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
-                                                 const uint32_t *__restrict__ entries,
-                                                 const Affine<F> *__restrict__ pts, uint32_t nb,
-                                                 uint32_t k1, Xyzz<F> *__restrict__ partials,
-                                                 Xyzz<F> *__restrict__ buckets)
+__device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets,
+                                            const uint32_t *__restrict__ entries,
+                                            const Affine<F> *__restrict__ pts, uint32_t nb,
+                                            uint32_t k1, Xyzz<F> *__restrict__ partials,
+                                            Xyzz<F> *__restrict__ buckets)
 {
     const uint32_t total = offsets[nb];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,6 +263,32 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
         buckets[b] = stx(acc);
     else
         partials[2ull * t + (first ? 0 : 1)] = stx(acc);
+}
+
+// Two register budgets for the same loop.  The compiler's own choice (160
+// registers for G1, 3 blocks of 128 threads per SM) is best for small grids; a
+// 4-block budget (128 registers, a few spills) hides more latency once the grid
+// fills the GPU several times over (measured 12% faster at 2^18..2^20 points,
+// slower at 2^16).  acc_run_t picks by grid size.
+template <class F>
+__global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
+                                                 const uint32_t *__restrict__ entries,
+                                                 const Affine<F> *__restrict__ pts, uint32_t nb,
+                                                 uint32_t k1, Xyzz<F> *__restrict__ partials,
+                                                 Xyzz<F> *__restrict__ buckets)
+{
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets);
+}
+
+template <class F>
+__global__ void __launch_bounds__(128, 4) k_acc_l1_occ4(const uint32_t *__restrict__ offsets,
+                                                         const uint32_t *__restrict__ entries,
+                                                         const Affine<F> *__restrict__ pts,
+                                                         uint32_t nb, uint32_t k1,
+                                                         Xyzz<F> *__restrict__ partials,
+                                                         Xyzz<F> *__restrict__ buckets)
+{
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets);
 }
 
 // One group of k2 pieces (spaced `stride` pieces apart) of one bucket; the
@@ -309,11 +337,17 @@ __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ off
 // --------------------------------------------------------------------------
 
 // buckets per thread of the first reduction level (log2): about 2^16 threads
-// (short dependent chains, enough warps), at most 16 buckets each
-__host__ __device__ constexpr int first_level_log2(uint32_t m)
+// (short dependent chains, enough warps), at most 16 buckets each.  The
+// environment variable NKR_B200_REDUCE_L2 sets it for tuning experiments.
+int first_level_log2(uint32_t m)
 {
+    static const int forced = [] {
+        const char *e = std::getenv("NKR_B200_REDUCE_L2");
+        return e ? std::atoi(e) : -1;
+    }();
     int lg = 0;
     while ((uint64_t(1) << (lg + 1)) <= m) ++lg;
+    if (forced >= 0) return forced < lg ? forced : lg;
     return lg <= 16 ? 0 : lg - 16 > 4 ? 4 : lg - 16;
 }
 
@@ -587,6 +621,22 @@ int build_windows_t(MsmBases &b, cudaStream_t st)
     return NKR_B200_OK;
 }
 
+// SMs of the current device (cached per device; a device attribute query is
+// allowed while a stream is being captured)
+int sm_count()
+{
+    static int cached[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
 template <class F>
 int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
@@ -595,9 +645,12 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     const uint64_t segs = sh.segments_max();
     const uint32_t *offsets = s.offsets.as<uint32_t>();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[0], st));
-    k_acc_l1<F><<<blocks_for(segs, 128), 128, 0, st>>>(offsets, s.entries.as<uint32_t>(),
-                                                       bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
-                                                       a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
+    const unsigned acc_blocks = blocks_for(segs, 128);
+    auto kernel = k_acc_l1<F>;
+    if constexpr (std::is_same<F, Fq>::value) // the G2 loop needs its full register budget
+        if (acc_blocks > 3u * unsigned(sm_count())) kernel = k_acc_l1_occ4<F>;
+    kernel<<<acc_blocks, 128, 0, st>>>(offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb,
+                                       uint32_t(sh.k1), a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[1], st));
     // fix-up levels: inputs spaced `stride` pieces apart, groups of k2; one

@@ -149,15 +149,35 @@ ProveSlot::~ProveSlot()
     if (pinned_out) cudaFreeHost(pinned_out);
 }
 
+// Stream priority of a key's slots: smaller circuits run at higher priority.
+// Levels above the lowest (B200 has five): 2^16 and below 5, 2^17 4, 2^18 3,
+// 2^19..2^20 2, 2^21..2^22 1, 2^23 and up 0.  When proofs of several keys share
+// the GPU (batches, the request server) the block scheduler then starts the
+// blocks of shorter proofs first, so a small request is not held behind a large
+// one; a proof alone runs as before.
+static int slot_stream_priority(int logn)
+{
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const int levels = least - greatest; // priorities run from least (0) down to greatest (< 0)
+    const int above = logn <= 16 ? 5 : logn == 17 ? 4 : logn == 18 ? 3 : logn <= 20 ? 2 : logn <= 22 ? 1 : 0;
+    return least - (above < levels ? above : levels);
+}
+
 int slot_add(nkr_b200_key *key)
 {
     NKR_CUDA(cudaSetDevice(key->ctx->device));
     auto slot = std::make_unique<ProveSlot>();
     ProveSlot *sl = slot.get();
-    // (a higher priority for the main stream was measured slower: the H chain
-    // finishes early but the H MSM then crowds out the witness MSMs)
+    // one priority for all streams of a slot (a higher priority for the main
+    // stream alone was measured slower: the H chain finishes early but the H MSM
+    // then crowds out the witness MSMs)
+    const int prio = slot_stream_priority(key->logn);
     for (int k = 0; k < kNumMsm; ++k) {
-        NKR_CUDA(cudaStreamCreateWithFlags(&sl->st[k], cudaStreamNonBlocking));
+        NKR_CUDA(cudaStreamCreateWithPriority(&sl->st[k], cudaStreamNonBlocking, prio));
         NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_done[k], cudaEventDisableTiming));
     }
     NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_z, cudaEventDisableTiming));

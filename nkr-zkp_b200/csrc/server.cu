@@ -3,10 +3,12 @@
 // The reference proves one request at a time per process (app/prove.cpp:70-88;
 // its bench runs one process per GPU, scripts/bench/runner.py:420-428).  Here
 // one server owns a set of prepared keys; callers submit (key, witness) requests
-// from any thread and wait for them.  A scheduler thread
+// from any thread and wait for them.  Slot streams carry a priority by circuit
+// size (prover.cu, slot_stream_priority), so among the requests in flight the
+// block scheduler serves smaller proofs first.  A scheduler thread
 //   - admits the oldest waiting request whose key has a free prove slot, adding
 //     a slot to the key when free HBM admits one (kServerHeadroom kept free) and
-//     the key has fewer than max_slots_per_key,
+//     the key has fewer than its slot cap (key_slot_cap),
 //   - uploads the witness and replays the slot's captured prove graph on the
 //     slot's streams, so requests of different keys (and several of one key)
 //     overlap on the device while earlier ones are still running,
@@ -14,6 +16,7 @@
 //     wakes their waiters.
 // A request's result does not depend on what else is in flight: every slot has
 // its own buffers and the resident key data is read only.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -87,6 +90,17 @@ double ms_since(const Clock::time_point &a, const Clock::time_point &b)
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+// Requests of one key that may be on the GPU at once.  A proof of 2^19 rows or
+// more fills the GPU by itself; running several of them side by side makes
+// every one of them finish late (processor sharing among equal jobs: two
+// together both end at about twice the time, one after the other end at one
+// and two times), so such keys prove one request at a time and the rest wait in
+// arrival order.  Smaller keys take up to max_slots_per_key.
+int key_slot_cap(const nkr_b200_server *sv, const nkr_b200_key *key)
+{
+    return key->logn >= 19 ? 1 : sv->max_slots_per_key;
+}
+
 // Start request r on a free slot of its key; returns false when none can be had.
 bool try_start(nkr_b200_server *sv, Request *r)
 {
@@ -97,7 +111,7 @@ bool try_start(nkr_b200_server *sv, Request *r)
             free_slot = &s;
             break;
         }
-    if (!free_slot && int(ks.slots.size()) < sv->max_slots_per_key) {
+    if (!free_slot && int(ks.slots.size()) < key_slot_cap(sv, ks.key)) {
         // the key's existing slots first (slot 0 is always resident), then new
         // ones while free HBM admits them
         nkr_b200_key *key = ks.key;

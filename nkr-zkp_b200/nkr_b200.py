@@ -86,6 +86,8 @@ _SIGS = {
     "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
                                             ctypes.POINTER(RawProofC)]),
     "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
+    "nkr_b200_ntt_device": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, _U64, _VP,
+                                           ctypes.POINTER(ctypes.c_float)]),
     "nkr_b200_server_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "nkr_b200_server_add_key": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_int)]),
     "nkr_b200_server_submit": (ctypes.c_int, [_VP, ctypes.c_int, _VP, ctypes.POINTER(_U64)]),
@@ -263,6 +265,14 @@ class Context:
         d = _fr(data).copy()
         _check(_lib.nkr_b200_ntt(self.h, op, _ptr(d), d.size // 4), f"ntt op {op}")
         return d.reshape(-1, 4)
+
+    def ntt_device(self, op, in_ptr, out_ptr, n, stream_ptr=None, timed=False):
+        """Domain op on device vectors (result in out_ptr, in_ptr overwritten); with
+        timed, waits and returns the device milliseconds."""
+        ms = ctypes.c_float()
+        _check(_lib.nkr_b200_ntt_device(self.h, op, in_ptr, out_ptr, n, stream_ptr,
+                                        ctypes.byref(ms) if timed else None), f"ntt_device op {op}")
+        return ms.value if timed else None
 
     def spmv(self, rows, cols, row_ptr, col_idx, values, z):
         y = np.zeros((rows, 4), np.uint64)

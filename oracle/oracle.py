@@ -403,6 +403,49 @@ def ref_available():
     return os.path.exists(REF_PATH)
 
 
+REFCUDA_PATH = os.path.join(HERE, "_ref", "libnkr_ref_cuda.so")
+
+
+def refcuda_available():
+    return os.path.exists(REFCUDA_PATH)
+
+
+class RefCuda:
+    """The reference's own CUDA backend (CudaBackend::prepare / prove,
+    protocols/groth16/backends/cuda/src/groth16_backend.cu:214-279) rebuilt for
+    sm_100a (oracle/ref_cuda_shim.cu).  Keys must be affine-normalised."""
+
+    def __init__(self):
+        if not refcuda_available():
+            raise FileNotFoundError(f"{REFCUDA_PATH} missing; run `make -C oracle refcuda`")
+        self.lib = ctypes.CDLL(REFCUDA_PATH)
+        self.lib.refcuda_last_error.restype = ctypes.c_char_p
+        self.lib.refcuda_open.restype = _VP
+        self.lib.refcuda_open.argtypes = [_VP] + [_VP] * 5
+        self.lib.refcuda_prove.argtypes = [_VP, _VP, _VP, _VP, ctypes.POINTER(ctypes.c_double)]
+        self.lib.refcuda_close.argtypes = [_VP]
+
+    def open(self, r1cs, pk):
+        c = Oracle._circuit(None, r1cs)
+        q = [_arr(pk[k]) for k in ("a_query", "b_g1_query", "b_g2_query", "l_query", "h_query")]
+        h = self.lib.refcuda_open(ctypes.byref(c), *[_p(x) for x in q])
+        if not h:
+            raise RuntimeError(self.lib.refcuda_last_error().decode())
+        return h
+
+    def prove(self, h, witness):
+        """(g1 affine [4, 8], g2 affine [16], host wall ms of the reference's prove)"""
+        g1 = np.zeros(32, np.uint64)
+        g2 = np.zeros(16, np.uint64)
+        ms = ctypes.c_double()
+        if self.lib.refcuda_prove(h, _p(_arr(witness)), _p(g1), _p(g2), ctypes.byref(ms)) != 0:
+            raise RuntimeError(self.lib.refcuda_last_error().decode())
+        return g1.reshape(4, 8), g2, ms.value
+
+    def close(self, h):
+        self.lib.refcuda_close(h)
+
+
 DROPIN_PATH = os.path.join(HERE, "_ref", "libnkr_ref_b200.so")
 
 

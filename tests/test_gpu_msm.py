@@ -183,3 +183,39 @@ def test_msm_linearity_at_2_20(ctx, orc, rng):
     assert np.array_equal(rs[:8], want)
     b.free()
     del ai
+
+
+def _sparse_witness_scalars(n, rng):
+    """10% uniform, 30% zero, 60% uniformly one of {zero, one, small < 2^16}."""
+    small = np.stack([O.fr_mont(v) for v in range(1 << 16)])
+    out = np.zeros((n, 4), np.uint64)
+    n_uni, n_zero = n // 10, (3 * n) // 10
+    out[:n_uni] = O.random_fr(n_uni, rng)
+    rest = n - n_uni - n_zero
+    cat = rng.integers(0, 3, rest)
+    vals = np.where(cat == 0, 0, np.where(cat == 1, 1, rng.integers(0, 1 << 16, rest)))
+    out[n_uni + n_zero:] = small[vals]
+    return out[rng.permutation(n)]
+
+
+@pytest.mark.parametrize("group,logn,mix", [(1, 22, "uniform"), (1, 22, "sparse"), (1, 20, "sparse"),
+                                            (2, 18, "uniform"), (2, 18, "sparse")])
+def test_msm_full_size_equals_scalar_sum(ctx, orc, rng, group, logn, mix):
+    """The operator-bench sizes with distinct bases P_i = k_i G: the MSM must equal
+    (sum_i s_i k_i) G, computed by the oracle (one scalar multiplication)."""
+    n = 1 << logn
+    gen = orc.g1_generator() if group == 1 else orc.g2_generator()
+    gen_jac = O.affine_to_jac(group, gen[None])[0]
+    ks = O.random_fr(n, rng)
+    bases = ctx.group_op(group, 2, np.tile(gen_jac, (n, 1)), ks)
+    for j in rng.integers(0, n, 3):   # spot-check the bases themselves
+        assert np.array_equal(bases[j], O.affine_to_jac(group, orc.mul_affine(group, gen, ks[j])[None])[0])
+    sc = O.random_fr(n, rng) if mix == "uniform" else _sparse_witness_scalars(n, rng)
+    ints = lambda a: [int.from_bytes(row.tobytes(), "little") for row in a]  # noqa: E731
+    t = sum(a * b for a, b in zip(ints(sc), ints(ks))) * pow(2, -512, O.R) % O.R
+    want = O.affine_to_jac(group, orc.mul_affine(group, gen, O.fr_mont(t))[None])[0]
+    b = nk.MsmBases(ctx, group, bases)
+    del bases
+    got, _ = b.run(sc)
+    b.free()
+    assert np.array_equal(got, want)

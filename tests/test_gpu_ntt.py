@@ -29,7 +29,7 @@ def test_domain_ops_golden(ctx):
         assert O.sha256_arr(ctx.ntt(int(op), x)) == digest, f"op {op}"
 
 
-@pytest.mark.parametrize("logn", [20, 22])
+@pytest.mark.parametrize("logn", [20, 22, 24])
 def test_large_round_trips_and_spot_values(ctx, logn, rng):
     """Size-independent properties at the benchmark sizes: inverse pairs are
     identities, linearity holds, and sampled outputs equal the definition
@@ -59,3 +59,50 @@ def test_large_round_trips_and_spot_values(ctx, logn, rng):
                 acc = (acc + a * p) % O.R
                 p = p * wj % O.R
             assert O.fr_int(f[j]) == acc
+
+
+@pytest.mark.parametrize("logn", [16, 24])
+def test_sparse_input_matches_definition_at_full_size(ctx, logn, rng):
+    """FFT and cosetFFT of a vector with 48 nonzero coefficients, checked at sampled
+    outputs against sum_i a_i w^(ij) (and a_i (g w^j)^i for the coset), any size."""
+    n = 1 << logn
+    x = np.zeros((n, 4), np.uint64)
+    pos = rng.choice(n, 48, replace=False)
+    x[pos] = O.random_fr(48, rng)
+    w = pow(pow(5, (O.R - 1) >> 28, O.R), 1 << (28 - logn), O.R)
+    nz = [(int(i), O.fr_int(x[i])) for i in pos]
+    f, c = ctx.ntt(0, x), ctx.ntt(2, x)
+    for j in [0, 1, n - 1] + [int(v) for v in rng.integers(0, n, 5)]:
+        wj = pow(w, j, O.R)
+        assert O.fr_int(f[j]) == sum(a * pow(wj, i, O.R) for i, a in nz) % O.R
+        gw = 5 * wj % O.R
+        assert O.fr_int(c[j]) == sum(a * pow(gw, i, O.R) for i, a in nz) % O.R
+
+
+@pytest.mark.parametrize("logn", [4, 16, 20])
+def test_device_entry_point_equals_host_entry_point(ctx, logn, rng):
+    import torch
+    n = 1 << logn
+    x = O.random_fr(n, rng)
+    xd = torch.from_numpy(x.view(np.int64).reshape(-1)).to("cuda:0")
+    for op in range(5):
+        work, out = xd.clone(), torch.empty_like(xd)
+        stream = torch.cuda.current_stream().cuda_stream   # orders the op after the clone
+        ms = ctx.ntt_device(op, work.data_ptr(), out.data_ptr(), n, stream_ptr=stream, timed=True)
+        assert ms > 0
+        got = out.cpu().numpy().view(np.uint64).reshape(n, 4)
+        assert np.array_equal(got, ctx.ntt(op, x)), f"op {op}"
+
+
+def test_device_entry_point_rejects_bad_buffers(ctx):
+    import torch
+    import nkr_b200 as nk
+    n = 1 << 10
+    xd = torch.zeros(4 * n * 2, dtype=torch.int64, device="cuda:0")
+    with pytest.raises(nk.B200Error, match="overlap"):
+        ctx.ntt_device(0, xd.data_ptr(), xd.data_ptr() + 64, n)
+    host = np.zeros((n, 4), np.uint64)
+    with pytest.raises(nk.B200Error, match="device memory"):
+        ctx.ntt_device(0, host.ctypes.data, xd.data_ptr() + n * 32, n)
+    with pytest.raises(nk.B200Error, match="power of two"):
+        ctx.ntt_device(0, xd.data_ptr(), xd.data_ptr() + n * 32, 1000)
