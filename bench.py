@@ -819,7 +819,8 @@ def run_kernels(args):
                              (1, 20, "sparse"), (1, 22, "uniform"), (1, 22, "sparse"),
                              (2, 18, "uniform"), (1, 18, "uniform")]:
         # the 2^18 G1 case is the small profiling case (run only when named)
-        if (want is None and logn != 18) or (want is not None and f"msm.g{group}.{mix}.{logn}" in want):
+        if (want is None and (group, logn) != (1, 18)) or \
+                (want is not None and f"msm.g{group}.{mix}.{logn}" in want):
             rows.append(msm_case(group, logn, mix))
     clk = clocks.stop()
     line = {
