@@ -47,7 +47,13 @@ WORKLOADS = {
 }
 METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
 REF_SAMPLE = ("poseidon", 128, 2)  # 2^16 constraints
-TRAFFIC_PER_ENTRY = (390.744064e6 + 48.899328e6) / 3373063  # k_acc_l1<Fq>, 2^18 capture
+# DRAM read + write bytes per (point, digit) entry of the G1 accumulation kernel,
+# from an ncu capture at 2^18 points (a 2^20 capture would hold ~6 GB of keys on
+# the device); traffic grows with entries (one random base gather per entry)
+TRAFFIC_PER_ENTRY = (452.237056e6 + 26.803968e6) / 3932125   # 121.8 B per entry
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_acc_l1_g1 on the "
+                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 121.8 B "
+                  "per entry, scaled by this launch's entries")
 
 
 def _dist():
@@ -103,6 +109,18 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def replica_ms_per_proof(total_ms, proofs, world, dist=None, device="cpu"):
+    """Whole-job milliseconds per proof of `world` independent replicas that each
+    proved `proofs` times in `total_ms`: the slowest rank's time over all ranks'
+    proofs (one MAX all-reduce, the only collective of the replica path)."""
+    if dist is not None:
+        import torch
+        t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms / (proofs * world)
 
 
 def _measured_peaks():
@@ -292,12 +310,8 @@ def run_b200(args):
     print(f"[bench] launches in the timed region: {launches} ({launches // args.steps} per prove)",
           file=sys.stderr)
     clk = clocks.stop()
-    dev_ms = sum(s["total_ms"] for s in stage)
-    if dist is not None:
-        t = torch.tensor([dev_ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
-    value = dev_ms / (args.steps * world)
+    value = replica_ms_per_proof(sum(s["total_ms"] for s in stage), args.steps, world, dist,
+                                 f"cuda:{device}")
 
     # ---- end to end through the C ABI from pinned host memory -------------------
     rs = _seeded_toxic(5)[:2]
@@ -308,11 +322,7 @@ def run_b200(args):
         be.blind(raw, rs[0], rs[1])
         if i >= args.warmup:
             e2e.append((time.perf_counter() - t1) * 1e3)
-    e2e_ms = sum(e2e) / len(e2e)
-    if dist is not None:
-        t = torch.tensor([sum(e2e)], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item()) / (len(e2e) * world)
+    e2e_ms = replica_ms_per_proof(sum(e2e), len(e2e), world, dist, f"cuda:{device}")
     h2d = r1.cols * 32 + 576 + 64
     d2h = 576 + 384
 
@@ -341,8 +351,8 @@ def run_b200(args):
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         # DRAM bytes per entry from an ncu capture of this kernel at 2^18 (read + write
         # 439.6 MB over 3,373,063 entries), scaled to this launch's entries
-        traffic = round(st["entries"] * TRAFFIC_PER_ENTRY)
-        roof = {"bound": "int", "kernel": "k_acc_l1<Fq> (G1 bucket accumulation)",
+        traffic = round(st["entries"] * TRAFFIC_PER_ENTRY) if TRAFFIC_PER_ENTRY else None
+        roof = {"bound": "int", "kernel": "k_acc_l1_g1 (G1 bucket accumulation)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),
                 "unit": "G Fq-mul/s", "frac": round(achieved / muls_peak, 3),
                 "peak_source": "measured: nkr_b200_bench_mul register-resident Fq Montgomery "
@@ -358,8 +368,7 @@ def run_b200(args):
                         "frac": round(algo_bytes / (acc_ms * 1e-3) / 1e9 / hbm_peak, 4),
                         "algorithmic_bytes": algo_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
                 "traffic": traffic, "traffic_unit": "bytes per launch",
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 2^18, "
-                                  "130.3 B per entry, scaled by entries"}
+                "traffic_source": TRAFFIC_SOURCE}
         mb.free()
 
     # ---- CPU baseline (rank 0, N = 1 only) --------------------------------------

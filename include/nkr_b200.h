@@ -110,6 +110,23 @@ void nkr_b200_key_free(nkr_b200_key *key);
 /* device bytes the key holds */
 uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key);
 
+/* Proving-key artifacts in the reference's BinaryArchive format ("LKZ1" v1; the
+ * layout of read_proving_key / write_proving_key, common/src/io.cpp:54-61), with
+ * no limit on vector size: the reference's BinaryArchive refuses vectors above
+ * 1 GiB (common/include/binary_archive.hpp:19, 76-77, 89-90), i.e. every key from
+ * 2^24 constraints up.  nkr_b200_prepare_file memory-maps the file and prepares
+ * the key from the mapped queries (no host copy; the same checks as
+ * nkr_b200_prepare, plus the file's structure and each query's length against the
+ * circuit).  nkr_b200_pk_file_info returns the point counts a file holds (rows =
+ * h_query, cols = the other queries) without touching a GPU.
+ * nkr_b200_write_proving_key writes the same format (queries G1/G2 Jacobian:
+ * a, b_g1, b_g2, l with cols points, h with rows points). */
+int nkr_b200_prepare_file(nkr_b200_ctx *ctx, const nkr_b200_circuit *circuit, const char *pk_path,
+                          nkr_b200_key **out);
+int nkr_b200_pk_file_info(const char *path, uint64_t *rows, uint64_t *cols);
+int nkr_b200_write_proving_key(const char *path, const nkr_b200_proving_key *pk, uint64_t rows,
+                               uint64_t cols);
+
 /* Replaces Backend::prove (backend.hpp:24-28; CPU backends/cpu/src/backend.cpp:156-201,
  * CUDA groth16_backend.cu:242-279).  witness: Fr[cols] host memory. */
 int nkr_b200_prove(nkr_b200_key *key, const void *witness, uint64_t n,

@@ -60,74 +60,139 @@ __device__ __forceinline__ Xyzz<F> xyzz_from_affine_dbl(const Affine<F> &p)
     return r;
 }
 
-// 2 * P (dbl-2008-s-1)
+// x = a b, y = c d.  Fields with a paired product (field52.cuh) overload this so
+// the two independent products share one call and interleave their chains.
+template <class F>
+__device__ __forceinline__ void mul2(const F &a, const F &b, const F &c, const F &d, F &x, F &y)
+{
+    x = a * b;
+    y = c * d;
+}
+
+// 2 * P (dbl-2008-s-1): 6M + 3S, as four independent pairs and one single
+// product where the field has a paired product
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_dbl(const Xyzz<F> &p)
 {
     if (p.is_inf() || p.y.is_zero()) return Xyzz<F>::inf();
     const F u = dbl(p.y);
-    const F v = sqr(u);
-    const F w = u * v;
-    const F s = p.x * v;
-    const F m = times3(sqr(p.x));
     Xyzz<F> r;
-    r.x = sqr(m) - dbl(s);
-    r.y = m * (s - r.x) - w * p.y;
-    r.zz = v * p.zz;
-    r.zzz = w * p.zzz;
+    if constexpr (HasPairedMul<F>::value) {
+        F v, xx, w, s, my, wy;
+        mul2(u, u, p.x, p.x, v, xx);
+        mul2(u, v, p.x, v, w, s);
+        mul2(v, p.zz, w, p.zzz, r.zz, r.zzz);
+        const F m = times3(xx);
+        r.x = sqr(m) - dbl(s);
+        mul2(m, s - r.x, w, p.y, my, wy);
+        r.y = my - wy;
+    } else {
+        const F v = sqr(u);
+        const F w = u * v;
+        const F s = p.x * v;
+        const F m = times3(sqr(p.x));
+        r.x = sqr(m) - dbl(s);
+        r.y = m * (s - r.x) - w * p.y;
+        r.zz = v * p.zz;
+        r.zzz = w * p.zzz;
+    }
     return r;
 }
 
-// acc + q for affine q (madd-2008-s); q may be infinity
+// acc + q for affine q (madd-2008-s): 8M + 2S, as five independent pairs where
+// the field has a paired product; q may be infinity
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F> &acc, const Affine<F> &q)
 {
     if (q.is_inf()) return acc;
     if (acc.is_inf()) return {q.x, q.y, F::one(), F::one()};
-    const F u2 = q.x * acc.zz;
-    const F s2 = q.y * acc.zzz;
-    const F p = u2 - acc.x;
-    const F r = s2 - acc.y;
-    if (p.is_zero()) {
-        if (r.is_zero()) return xyzz_from_affine_dbl(q);
-        return Xyzz<F>::inf();
+    if constexpr (HasPairedMul<F>::value) {
+        F u2, s2;
+        mul2(q.x, acc.zz, q.y, acc.zzz, u2, s2);
+        const F p = u2 - acc.x;
+        const F r = s2 - acc.y;
+        if (p.is_zero()) {
+            if (r.is_zero()) return xyzz_from_affine_dbl(q);
+            return Xyzz<F>::inf();
+        }
+        F pp, rr, ppp, qq, y1ppp, ry;
+        mul2(p, p, r, r, pp, rr);
+        mul2(p, pp, acc.x, pp, ppp, qq);
+        Xyzz<F> o;
+        mul2(acc.zzz, ppp, acc.y, ppp, o.zzz, y1ppp);
+        o.x = rr - ppp - dbl(qq);
+        mul2(r, qq - o.x, acc.zz, pp, ry, o.zz);
+        o.y = ry - y1ppp;
+        return o;
+    } else {
+        const F u2 = q.x * acc.zz;
+        const F s2 = q.y * acc.zzz;
+        const F p = u2 - acc.x;
+        const F r = s2 - acc.y;
+        if (p.is_zero()) {
+            if (r.is_zero()) return xyzz_from_affine_dbl(q);
+            return Xyzz<F>::inf();
+        }
+        const F pp = sqr(p);
+        const F ppp = p * pp;
+        const F qq = acc.x * pp;
+        Xyzz<F> o;
+        o.x = sqr(r) - ppp - dbl(qq);
+        o.y = r * (qq - o.x) - acc.y * ppp;
+        o.zz = acc.zz * pp;
+        o.zzz = acc.zzz * ppp;
+        return o;
     }
-    const F pp = sqr(p);
-    const F ppp = p * pp;
-    const F qq = acc.x * pp;
-    Xyzz<F> o;
-    o.x = sqr(r) - ppp - dbl(qq);
-    o.y = r * (qq - o.x) - acc.y * ppp;
-    o.zz = acc.zz * pp;
-    o.zzz = acc.zzz * ppp;
-    return o;
 }
 
-// a + b (add-2008-s)
+// a + b (add-2008-s): 12M + 2S, as seven independent pairs where the field has a
+// paired product
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F> &a, const Xyzz<F> &b)
 {
     if (a.is_inf()) return b;
     if (b.is_inf()) return a;
-    const F u1 = a.x * b.zz;
-    const F u2 = b.x * a.zz;
-    const F s1 = a.y * b.zzz;
-    const F s2 = b.y * a.zzz;
-    const F p = u2 - u1;
-    const F r = s2 - s1;
-    if (p.is_zero()) {
-        if (r.is_zero()) return xyzz_dbl(a);
-        return Xyzz<F>::inf();
+    if constexpr (HasPairedMul<F>::value) {
+        F u1, u2, s1, s2;
+        mul2(a.x, b.zz, b.x, a.zz, u1, u2);
+        mul2(a.y, b.zzz, b.y, a.zzz, s1, s2);
+        const F p = u2 - u1;
+        const F r = s2 - s1;
+        if (p.is_zero()) {
+            if (r.is_zero()) return xyzz_dbl(a);
+            return Xyzz<F>::inf();
+        }
+        F pp, rr, ppp, qq, zz_ab, zzz_ab, ry, s1ppp;
+        mul2(p, p, r, r, pp, rr);
+        mul2(p, pp, u1, pp, ppp, qq);
+        mul2(a.zz, b.zz, a.zzz, b.zzz, zz_ab, zzz_ab);
+        Xyzz<F> o;
+        o.x = rr - ppp - dbl(qq);
+        mul2(r, qq - o.x, s1, ppp, ry, s1ppp);
+        o.y = ry - s1ppp;
+        mul2(zz_ab, pp, zzz_ab, ppp, o.zz, o.zzz);
+        return o;
+    } else {
+        const F u1 = a.x * b.zz;
+        const F u2 = b.x * a.zz;
+        const F s1 = a.y * b.zzz;
+        const F s2 = b.y * a.zzz;
+        const F p = u2 - u1;
+        const F r = s2 - s1;
+        if (p.is_zero()) {
+            if (r.is_zero()) return xyzz_dbl(a);
+            return Xyzz<F>::inf();
+        }
+        const F pp = sqr(p);
+        const F ppp = p * pp;
+        const F qq = u1 * pp;
+        Xyzz<F> o;
+        o.x = sqr(r) - ppp - dbl(qq);
+        o.y = r * (qq - o.x) - s1 * ppp;
+        o.zz = a.zz * b.zz * pp;
+        o.zzz = a.zzz * b.zzz * ppp;
+        return o;
     }
-    const F pp = sqr(p);
-    const F ppp = p * pp;
-    const F qq = u1 * pp;
-    Xyzz<F> o;
-    o.x = sqr(r) - ppp - dbl(qq);
-    o.y = r * (qq - o.x) - s1 * ppp;
-    o.zz = a.zz * b.zz * pp;
-    o.zzz = a.zzz * b.zzz * ppp;
-    return o;
 }
 
 template <class F>

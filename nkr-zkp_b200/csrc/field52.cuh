@@ -105,72 +105,136 @@ __device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
 #define NKR_MUL52_ATTR __forceinline__
 #endif
 
-// a b 2^-260 mod p, canonical; needs a b < 2^260 p (true for a, b < 4p)
-__device__ NKR_MUL52_ATTR Fq52 mul52(const Fq52 &a, const Fq52 &b)
+// N independent products r[k] = a[k] b[k] 2^-260 mod p, canonical; each needs
+// a b < 2^260 p (true for a, b < 4p).  The N computations share no data, so the
+// scheduler interleaves their dependency chains (the word-serial reduction is
+// one long chain per product).
+template <int N>
+__device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *const *b, Fq52 *const *r)
 {
     using namespace f52;
-    double ad[5], bd[5], pd[5];
+    double ad[N][5], bd[N][5], pd[5];
 #pragma unroll
-    for (int i = 0; i < 5; ++i) {
-        ad[i] = to_double(a.l[i]);
-        bd[i] = to_double(b.l[i]);
-        pd[i] = double(p_limb(i)); // exact, folded at compile time
-    }
-    uint64_t C[10];
+    for (int i = 0; i < 5; ++i) pd[i] = double(p_limb(i)); // exact, folded at compile time
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            ad[k][i] = to_double(a[k]->l[i]);
+            bd[k][i] = to_double(b[k]->l[i]);
+        }
+    uint64_t C[N][10];
     uint64_t bias[10];
 #pragma unroll
-    for (int k = 0; k < 10; ++k) {
-        C[k] = 0;
-        bias[k] = 0;
+    for (int j = 0; j < 10; ++j) {
+        bias[j] = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) C[k][j] = 0;
     }
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
         for (int j = 0; j < 5; ++j) {
-            uint64_t lo, hi;
-            mul_wide(ad[i], bd[j], lo, hi);
-            C[i + j] += lo;
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                uint64_t lo, hi;
+                mul_wide(ad[k][i], bd[k][j], lo, hi);
+                C[k][i + j] += lo;
+                C[k][i + j + 1] += hi;
+            }
             bias[i + j] += kBias52;
-            C[i + j + 1] += hi;
             bias[i + j + 1] += kBias104;
         }
     const double pinv = double(kPinv);
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
-        uint64_t t = C[i] - bias[i]; // the column's integer value
-        uint64_t qlo, qhi;
-        mul_wide(to_double(t & kMask), pinv, qlo, qhi);
-        const double q = __longlong_as_double(static_cast<long long>(qlo)) - 0x1p52;
-        uint64_t lo, hi;
-        mul_wide(q, pd[0], lo, hi);
-        t += lo - kBias52; // now 0 mod 2^52
-        C[i + 1] += hi + (t >> 52);
+        uint64_t t[N];
+        double q[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            t[k] = C[k][i] - bias[i]; // the column's integer value
+            uint64_t qlo, qhi;
+            mul_wide(to_double(t[k] & kMask), pinv, qlo, qhi);
+            q[k] = __longlong_as_double(static_cast<long long>(qlo)) - 0x1p52;
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            uint64_t lo, hi;
+            mul_wide(q[k], pd[0], lo, hi);
+            t[k] += lo - kBias52; // now 0 mod 2^52
+            C[k][i + 1] += hi + (t[k] >> 52);
+#pragma unroll
+            for (int j = 1; j < 5; ++j) {
+                mul_wide(q[k], pd[j], lo, hi);
+                C[k][i + j] += lo;
+                if (i + j + 1 < 10) C[k][i + j + 1] += hi;
+            }
+        }
         bias[i + 1] += kBias104;
 #pragma unroll
         for (int j = 1; j < 5; ++j) {
-            mul_wide(q, pd[j], lo, hi);
-            C[i + j] += lo;
             bias[i + j] += kBias52;
-            if (i + j + 1 < 10) {
-                C[i + j + 1] += hi;
-                bias[i + j + 1] += kBias104;
-            }
+            if (i + j + 1 < 10) bias[i + j + 1] += kBias104;
         }
     }
-    Fq52 r;
-    uint64_t carry = 0;
 #pragma unroll
-    for (int k = 5; k < 10; ++k) {
-        const uint64_t v = C[k] - bias[k] + carry;
-        r.l[k - 5] = v & kMask;
-        carry = v >> 52;
+    for (int k = 0; k < N; ++k) {
+        uint64_t carry = 0;
+#pragma unroll
+        for (int j = 5; j < 10; ++j) {
+            const uint64_t v = C[k][j] - bias[j] + carry;
+            r[k]->l[j - 5] = v & kMask;
+            carry = v >> 52;
+        }
+        sub_p_if_ge(r[k]->l); // the result is below 2p
     }
-    sub_p_if_ge(r.l); // the result is below 2p
+}
+
+__device__ NKR_MUL52_ATTR Fq52 mul52(Fq52 a, Fq52 b)
+{
+    Fq52 r;
+    const Fq52 *pa[1] = {&a}, *pb[1] = {&b};
+    Fq52 *pr[1] = {&r};
+    mul52_body<1>(pa, pb, pr);
     return r;
+}
+
+struct Fq52Pair {
+    Fq52 x, y;
+};
+
+// (a b, c d) in one call: two independent products with interleaved chains.
+// Operands and results travel by value so the call passes them in registers
+// (reference parameters would go through the thread's local-memory stack).
+__device__ NKR_MUL52_ATTR Fq52Pair mul52x2v(Fq52 a, Fq52 b, Fq52 c, Fq52 d)
+{
+    Fq52Pair r;
+    const Fq52 *pa[2] = {&a, &c}, *pb[2] = {&b, &d};
+    Fq52 *pr[2] = {&r.x, &r.y};
+    mul52_body<2>(pa, pb, pr);
+    return r;
+}
+
+__device__ __forceinline__ void mul52x2(const Fq52 &a, const Fq52 &b, const Fq52 &c, const Fq52 &d,
+                                        Fq52 &ab, Fq52 &cd)
+{
+    const Fq52Pair r = mul52x2v(a, b, c, d);
+    ab = r.x;
+    cd = r.y;
 }
 
 __device__ __forceinline__ Fq52 operator*(const Fq52 &a, const Fq52 &b) { return mul52(a, b); }
 __device__ __forceinline__ Fq52 sqr(const Fq52 &a) { return mul52(a, a); }
+// x = a b, y = c d (curve formulas issue independent products in pairs)
+__device__ __forceinline__ void mul2(const Fq52 &a, const Fq52 &b, const Fq52 &c, const Fq52 &d,
+                                     Fq52 &x, Fq52 &y)
+{
+    mul52x2(a, b, c, d, x, y);
+}
+template <>
+struct HasPairedMul<Fq52> {
+    static constexpr bool value = true;
+};
 
 __device__ __forceinline__ Fq52 operator+(const Fq52 &a, const Fq52 &b)
 {
@@ -236,15 +300,15 @@ __device__ __forceinline__ Fq2x52 neg(const Fq2x52 &a) { return {neg(a.c0), neg(
 __device__ __forceinline__ Fq2x52 dbl(const Fq2x52 &a) { return {dbl(a.c0), dbl(a.c1)}; }
 __device__ __forceinline__ Fq2x52 operator*(const Fq2x52 &a, const Fq2x52 &b)
 {
-    const Fq52 v0 = a.c0 * b.c0;
-    const Fq52 v1 = a.c1 * b.c1;
+    Fq52 v0, v1;
+    mul52x2(a.c0, b.c0, a.c1, b.c1, v0, v1);
     const Fq52 s = (a.c0 + a.c1) * (b.c0 + b.c1);
     return {v0 - v1, s - v0 - v1};
 }
 __device__ __forceinline__ Fq2x52 sqr(const Fq2x52 &a)
 {
-    const Fq52 p = (a.c0 + a.c1) * (a.c0 - a.c1);
-    const Fq52 q = a.c0 * a.c1;
+    Fq52 p, q;
+    mul52x2(a.c0 + a.c1, a.c0 - a.c1, a.c0, a.c1, p, q);
     return {p, q + q};
 }
 

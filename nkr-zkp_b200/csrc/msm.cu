@@ -108,7 +108,8 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
 // every G1 MSM buffer (bases, partials, buckets, reduction items) holds R'-domain
 // values in the 8 x 32-bit layout of Fq, converted at entry (bases) and exit
 // (result).  G2 arithmetic stays on the integer pipe (Fq2, R = 2^256): measured,
-// its FP64 form needs more than 255 registers and ran 30% slower.
+// its FP64 form (Fq2 products as three interleaved 52-bit products) needs all 255
+// registers and ran 34% slower at 2^18 points.
 // --------------------------------------------------------------------------
 
 template <class F>
@@ -265,11 +266,11 @@ __device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets
         partials[2ull * t + (first ? 0 : 1)] = stx(acc);
 }
 
-// Two register budgets for the same loop.  The compiler's own choice (160
-// registers for G1, 3 blocks of 128 threads per SM) is best for small grids; a
-// 4-block budget (128 registers, a few spills) hides more latency once the grid
-// fills the GPU several times over (measured 12% faster at 2^18..2^20 points,
-// slower at 2^16).  acc_run_t picks by grid size.
+// Level 1 kernels.  G1 (FP64 field, paired products passed by value) gets a
+// 3-blocks-per-SM register budget: measured against the compiler's own choice
+// (184 registers, 2 blocks) and a 4-block budget (128 registers, more spills),
+// it is the fastest from 2^16 to 2^20 points, uniform and sparse.  G2 keeps the
+// compiler's choice.
 template <class F>
 __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
                                                  const uint32_t *__restrict__ entries,
@@ -281,12 +282,12 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
 }
 
 template <class F>
-__global__ void __launch_bounds__(128, 4) k_acc_l1_occ4(const uint32_t *__restrict__ offsets,
-                                                         const uint32_t *__restrict__ entries,
-                                                         const Affine<F> *__restrict__ pts,
-                                                         uint32_t nb, uint32_t k1,
-                                                         Xyzz<F> *__restrict__ partials,
-                                                         Xyzz<F> *__restrict__ buckets)
+__global__ void __launch_bounds__(128, 3) k_acc_l1_g1(const uint32_t *__restrict__ offsets,
+                                                       const uint32_t *__restrict__ entries,
+                                                       const Affine<F> *__restrict__ pts,
+                                                       uint32_t nb, uint32_t k1,
+                                                       Xyzz<F> *__restrict__ partials,
+                                                       Xyzz<F> *__restrict__ buckets)
 {
     acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets);
 }
@@ -621,22 +622,6 @@ int build_windows_t(MsmBases &b, cudaStream_t st)
     return NKR_B200_OK;
 }
 
-// SMs of the current device (cached per device; a device attribute query is
-// allowed while a stream is being captured)
-int sm_count()
-{
-    static int cached[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (!cached[dev]) {
-        int n = 0;
-        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
-            n = 148;
-        cached[dev] = n;
-    }
-    return cached[dev];
-}
-
 template <class F>
 int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
@@ -645,12 +630,14 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     const uint64_t segs = sh.segments_max();
     const uint32_t *offsets = s.offsets.as<uint32_t>();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[0], st));
-    const unsigned acc_blocks = blocks_for(segs, 128);
-    auto kernel = k_acc_l1<F>;
-    if constexpr (std::is_same<F, Fq>::value) // the G2 loop needs its full register budget
-        if (acc_blocks > 3u * unsigned(sm_count())) kernel = k_acc_l1_occ4<F>;
-    kernel<<<acc_blocks, 128, 0, st>>>(offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb,
-                                       uint32_t(sh.k1), a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
+    if constexpr (std::is_same<F, Fq>::value)
+        k_acc_l1_g1<F><<<blocks_for(segs, 128), 128, 0, st>>>(
+            offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
+            a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
+    else
+        k_acc_l1<F><<<blocks_for(segs, 128), 128, 0, st>>>(
+            offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
+            a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[1], st));
     // fix-up levels: inputs spaced `stride` pieces apart, groups of k2; one

@@ -76,6 +76,12 @@ _SIGS = {
     "nkr_b200_backend_name": (ctypes.c_char_p, []),
     "nkr_b200_prepare": (ctypes.c_int, [_VP, ctypes.POINTER(Circuit), ctypes.POINTER(ProvingKey),
                                         ctypes.POINTER(_VP)]),
+    "nkr_b200_prepare_file": (ctypes.c_int, [_VP, ctypes.POINTER(Circuit), ctypes.c_char_p,
+                                             ctypes.POINTER(_VP)]),
+    "nkr_b200_pk_file_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_U64),
+                                             ctypes.POINTER(_U64)]),
+    "nkr_b200_write_proving_key": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ProvingKey),
+                                                  _U64, _U64]),
     "nkr_b200_key_free": (None, [_VP]),
     "nkr_b200_key_device_bytes": (_U64, [_VP]),
     "nkr_b200_prove": (ctypes.c_int, [_VP, _VP, _U64, ctypes.POINTER(RawProofC)]),
@@ -404,6 +410,18 @@ class Backend:
         self.cols = r1cs.cols
         self.rows = r1cs.rows
 
+    def prepare_file(self, r1cs, pk_path):
+        """prepare() from a proving-key artifact file (BinaryArchive, no 1 GiB limit)."""
+        c = r1cs.c_circuit()
+        h = _VP()
+        _check(_lib.nkr_b200_prepare_file(self.ctx.h, ctypes.byref(c), str(pk_path).encode(),
+                                          ctypes.byref(h)), "nkr_b200_prepare_file")
+        self.free()
+        self.key = h
+        self._keep = None
+        self.cols = r1cs.cols
+        self.rows = r1cs.rows
+
     def prove(self, witness, witness_ptr=None):
         raw = RawProofC()
         if witness_ptr is None:
@@ -482,6 +500,24 @@ def setup(ctx, r1cs, toxic):
                                "alpha_g1", "beta_g1", "delta_g1", "beta_g2", "delta_g2")}
     vk = {k: arrs[k] for k in ("ic", "gamma_g2", "delta_g2", "alpha_g1", "beta_g2")}
     return pk, vk
+
+
+def pk_file_info(path):
+    """(rows, cols) of a proving-key artifact file; reads no GPU."""
+    rows, cols = _U64(), _U64()
+    _check(_lib.nkr_b200_pk_file_info(str(path).encode(), ctypes.byref(rows), ctypes.byref(cols)),
+           "nkr_b200_pk_file_info")
+    return rows.value, cols.value
+
+
+def write_proving_key(path, pk, rows, cols):
+    """Writes a proving-key dict (libff Jacobian arrays) as a BinaryArchive artifact."""
+    keep = {k: np.ascontiguousarray(v, np.uint64) for k, v in pk.items()}
+    p = ProvingKey()
+    for name, _ in ProvingKey._fields_:
+        setattr(p, name, keep[name].ctypes.data)
+    _check(_lib.nkr_b200_write_proving_key(str(path).encode(), ctypes.byref(p), rows, cols),
+           "nkr_b200_write_proving_key")
 
 
 def prove_batch(backends, witnesses=None, witness_ptrs=None):

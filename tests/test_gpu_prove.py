@@ -76,7 +76,8 @@ def test_blind_matches_oracle_and_verifies(ctx, orc, ref, tmp_path):
 
 
 @pytest.mark.parametrize("kind,param,dens", [("poseidon", 3, 2), ("sql-aggregate", 2, 1),
-                                            ("matmul", 6, 1), ("fibonacci", 100, 0)])
+                                            ("matmul", 6, 1), ("fibonacci", 100, 0),
+                                            ("matmul", 32, 0)])   # the matmul-32 config: 2^16, full density
 def test_prove_matches_reference_live(ctx, ref, tmp_path, kind, param, dens):
     r1 = nk.generate(kind, param, dens, seed=31)
     pk_path, vk_path = tmp_path / "c.pk.bin", tmp_path / "c.vk.bin"

@@ -64,10 +64,12 @@ def test_gpu_setup_proof_verifies(ctx, ref, tmp_path):
     be.free()
 
 
-def test_full_size_2_20_prove(ctx, orc, ref, tmp_path):
-    """poseidon count=2048 at sparse density: 2^20 constraints and columns."""
-    r1 = nk.generate("poseidon", 2048, 2, seed=1)
-    assert r1.rows == 1 << 20
+@pytest.mark.parametrize("count,logn", [(2048, 20), (4096, 21)])
+def test_full_size_prove(ctx, orc, ref, tmp_path, count, logn):
+    """poseidon at sparse density, count 2048 (2^20 constraints and columns, the
+    headline size) and count 4096 (2^21, the full-prove config)."""
+    r1 = nk.generate("poseidon", count, 2, seed=1)
+    assert r1.rows == 1 << logn
     be, ok = _prove_and_verify(ctx, ref, r1, _toxic(4), tmp_path)
     assert ok
     az, bz, cz, h = be.intermediates()
