@@ -64,7 +64,7 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -76,13 +76,22 @@ class ClockSampler:
         self.out = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
 
     def start(self):
+        """Starts sampling every 50 ms and returns once the first sample is written,
+        so that even a short timed region that follows is sampled."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.out, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            self.out.flush()
+            if os.path.getsize(self.out.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:

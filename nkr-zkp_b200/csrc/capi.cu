@@ -329,9 +329,12 @@ int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_
     NKR_TRY(dz.alloc(std::max<uint64_t>(cols, 1) * 32, "spmv z"));
     NKR_TRY(dy.alloc(rows * 32, "spmv y"));
     NKR_CUDA(cudaMemcpyAsync(dz.p, z, cols * 32, cudaMemcpyHostToDevice, st));
+    DevBuf prod;
+    NKR_TRY(prod.alloc(std::max<uint64_t>(m.nu, 1) * 32, "spmv products"));
     const CsrDevice *mats[1] = {&m};
     Fr *ys[1] = {dy.as<Fr>()};
-    NKR_TRY(spmv_multi(mats, 1, dz.as<Fr>(), ys, st));
+    Fr *prods[1] = {prod.as<Fr>()};
+    NKR_TRY(spmv_multi(mats, 1, dz.as<Fr>(), ys, prods, st));
     NKR_CUDA(cudaMemcpyAsync(y, dy.p, rows * 32, cudaMemcpyDeviceToHost, st));
     NKR_CUDA(cudaStreamSynchronize(st));
     return NKR_B200_OK;

@@ -337,10 +337,13 @@ __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ off
 // bucket reduction: sum_b b * S_b per set, then + sum_b S_b
 // --------------------------------------------------------------------------
 
-// buckets per thread of the first reduction level (log2): about 2^16 threads
-// (short dependent chains, enough warps), at most 16 buckets each.  The
-// environment variable NKR_B200_REDUCE_L2 sets it for tuning experiments.
-int first_level_log2(uint32_t m)
+// Buckets per thread of the first reduction level (log2).  The block levels
+// that follow are latency bound (dependent additions), so the first level leaves
+// about 128 x BS items: the next level is then one wave of 128 blocks (at most one
+// 256-thread block per SM fits) and a single final block.  Measured fastest for
+// G1 (BS 256) at 2^15, 2^16 and 2^19 buckets and G2 (BS 128) at 2^15 and 2^16.
+// The environment variable NKR_B200_REDUCE_L2 sets it for tuning experiments.
+int first_level_log2(uint32_t m, int log2_bs)
 {
     static const int forced = [] {
         const char *e = std::getenv("NKR_B200_REDUCE_L2");
@@ -349,7 +352,8 @@ int first_level_log2(uint32_t m)
     int lg = 0;
     while ((uint64_t(1) << (lg + 1)) <= m) ++lg;
     if (forced >= 0) return forced < lg ? forced : lg;
-    return lg <= 16 ? 0 : lg - 16 > 4 ? 4 : lg - 16;
+    const int over = lg - (7 + log2_bs);
+    return over <= 0 ? 0 : over > 4 ? 4 : over;
 }
 
 // run += S_b for bucket b: S_b is empty, written whole by the level-1 kernel
@@ -665,7 +669,7 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
     // first level: bucket sums (few-piece buckets finished here), L buckets per thread
-    const int log2_l = first_level_log2(m);
+    const int log2_l = first_level_log2(m, kLog2BS);
     const uint32_t L = 1u << log2_l;
     const uint64_t items = uint64_t(sets) * m;
     k_reduce_first<F><<<blocks_for(items / L, 128), 128, 0, st>>>(
@@ -698,7 +702,8 @@ int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
 {
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     // first reduction level output: one item per L buckets (L as in acc_run_t)
-    const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B)) + 1;
+    constexpr int kLog2BS = sizeof(F) == sizeof(Fq) ? 8 : 7; // block size of acc_run_t's levels
+    const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B, kLog2BS)) + 1;
     NKR_TRY(a.partials.alloc(2 * std::max<uint64_t>(sh.segments_max(), 1) * sizeof(Xyzz<F>),
                              "msm partial sums"));
     NKR_TRY(a.buckets.alloc(uint64_t(sh.nb) * sizeof(Xyzz<F>), "msm buckets"));

@@ -202,6 +202,10 @@ int slot_add(nkr_b200_key *key)
     NKR_TRY(sl->h.alloc(key->rows * 32, "H"));
     NKR_TRY(sl->out.alloc(kOutBytes, "proof points"));
     bytes += sl->z.bytes + 4 * sl->az.bytes + sl->out.bytes;
+    for (int k = 0; k < 3; ++k) {
+        NKR_TRY(sl->spmv_prod[k].alloc(std::max<uint64_t>(key->mat[k].nu, 1) * 32, "SpMV products"));
+        bytes += sl->spmv_prod[k].bytes;
+    }
     if (cudaHostAlloc(&sl->pinned_out, kOutBytes + 384, cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         set_error("pinned host allocation failed");
@@ -222,7 +226,8 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed)
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[0], s0));
     const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
     Fr *ys[3] = {az, bz, cz};
-    NKR_TRY(spmv_multi(mats, 3, z, ys, s0));
+    Fr *prods[3] = {sl->spmv_prod[0].as<Fr>(), sl->spmv_prod[1].as<Fr>(), sl->spmv_prod[2].as<Fr>()};
+    NKR_TRY(spmv_multi(mats, 3, z, ys, prods, s0));
     NKR_CUDA(cudaEventRecord(sl->ev_z, s0));
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[1], s0));
     // witness MSMs on their own streams, overlapping the H chain; one digit sort
@@ -498,7 +503,8 @@ int key_intermediates(nkr_b200_key *key, void *az, void *bz, void *cz, void *h)
     // the SpMV is a pure function of the resident witness: recompute az, bz, cz
     const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
     Fr *ys[3] = {t, t + rows, t + 2 * rows};
-    NKR_TRY(spmv_multi(mats, 3, sl->z.as<Fr>(), ys, s0));
+    Fr *prods[3] = {sl->spmv_prod[0].as<Fr>(), sl->spmv_prod[1].as<Fr>(), sl->spmv_prod[2].as<Fr>()};
+    NKR_TRY(spmv_multi(mats, 3, sl->z.as<Fr>(), ys, prods, s0));
     // H is held in bit-reversed order; return it in natural order
     NKR_TRY(ntt_bitrev_permute(sl->h.as<Fr>(), t + 3 * rows, rows, nullptr, nullptr, s0));
     void *dst[4] = {az, bz, cz, h};
@@ -611,7 +617,8 @@ uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
     if (!key) return 0;
     uint64_t b = key->ntt.device_bytes() + key->pk_const.bytes + key->blind_io.bytes;
     for (int k = 0; k < 3; ++k)
-        b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].values.bytes;
+        b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].nu_col.bytes +
+             key->mat[k].nu_val.bytes;
     for (int k = 0; k < nkr::kNumMsm; ++k) b += key->bases[k].device_bytes();
     b += key->slot_bytes * key->slots.size();
     return b;

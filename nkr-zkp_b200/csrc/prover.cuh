@@ -54,6 +54,7 @@ struct ProveSlot {
     MsmSort sort_h;    // digit sort of H
     MsmAcc acc[kNumMsm];
     DevBuf z, az, bz, cz, h;
+    DevBuf spmv_prod[3]; // SpMV products of the non-unit terms, per matrix
     DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
     cudaStream_t st[kNumMsm] = {};
     cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};

@@ -45,3 +45,20 @@ def test_spmv_rejects_out_of_range_column(ctx):
     with pytest.raises(nk.B200Error):
         ctx.spmv(2, 3, np.array([0, 1, 2], np.uint32), np.array([0, 3], np.uint32),
                  np.zeros((2, 4), np.uint64), np.zeros((3, 4), np.uint64))
+
+
+@pytest.mark.parametrize("fill", ["all_unit", "all_zero", "all_general"])
+def test_spmv_single_coefficient_class(ctx, orc, rng, fill):
+    """Matrices whose terms all take one path: no non-unit terms (the product
+    launch is skipped), only skipped zero terms, or only general products."""
+    rows, cols = 700, 300
+    rp, ci, vals = _random_csr(rng, rows, cols, 6)
+    if fill == "all_unit":
+        vals[:] = O.fr_mont(1)
+    elif fill == "all_zero":
+        vals[:] = 0
+    else:
+        vals[:] = O.random_fr(len(vals), rng)
+    z = O.random_fr(cols, rng)
+    got = ctx.spmv(rows, cols, rp, ci, vals, z)
+    assert np.array_equal(got, orc.spmv(rows, rp, ci, vals, z))
