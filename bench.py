@@ -771,6 +771,7 @@ def run_kernels(args):
         out = torch.empty_like(x)
         back = torch.empty_like(x)
         stream = torch.cuda.current_stream().cuda_stream  # the copies below run on it
+        shape = ctx.tune_ntt(n)  # builds the size's tables and tunes its tile shape
         for op, name, inv_op in ((0, "fft", 1), (1, "ifft", 0), (2, "coset_fft", 3), (3, "icoset_fft", 2)):
             ts = []
             for it in range(args.warmup + args.steps):
@@ -791,6 +792,7 @@ def run_kernels(args):
                          "frac_fr_mul_peak": round(muls / (ms * 1e-3) / fr_peak, 3),
                          "GB_per_s": round(byts / ms / 1e6, 1),
                          "frac_hbm": round(byts / (ms * 1e-3) / 1e9 / hbm_peak, 3),
+                         "tile": {"max_stages_per_pass": shape[0], "butterflies_per_thread": shape[1]},
                          "check": "inverse round trip bit-exact" if ok else "ROUND TRIP FAILED"})
         del x, work, out, back
 

@@ -226,6 +226,12 @@ int nkr_b200_msm_g2(nkr_b200_ctx *ctx, const void *bases, const void *scalars, u
  * the measured MSM time at that size class (0 when the size is not measured).
  * Replaces choose_window_bits (backends/cuda/src/groth16_backend.cu:17-25: 8, 11
  * or 13 bits by size), which has no tuner. */
+/* NTT tile shape for n = 2^k points, chosen on this device when the size's tables
+ * are built (the first NTT of that size, or prepare): every pass split with 7..10
+ * radix-2 stages per pass and 1, 2 or 4 butterflies per thread and stage is timed
+ * and the fastest kept (sizes below 2^14 and NKR_B200_AUTOTUNE=0 keep 10 and 1).
+ * The reference's NTT has fixed launch shapes (ntt/ntt.cuh:126-158). */
+int nkr_b200_tune_ntt(nkr_b200_ctx *ctx, uint64_t n, int *max_stages, int *bfly_per_thread);
 int nkr_b200_set_autotune(nkr_b200_ctx *ctx, int enable);
 int nkr_b200_tune_msm(nkr_b200_ctx *ctx, uint64_t n, int *window_bits, float *ms);
 

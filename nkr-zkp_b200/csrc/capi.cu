@@ -465,6 +465,20 @@ void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b)
     delete b;
 }
 
+int nkr_b200_tune_ntt(nkr_b200_ctx *ctx, uint64_t n, int *max_stages, int *bfly_per_thread)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(max_stages && bfly_per_thread, "null argument");
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT size %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)n);
+    const NttTables *T;
+    NKR_TRY(get_tables(ctx, logn, &T));
+    *max_stages = T->max_stages;
+    *bfly_per_thread = T->bfly_per_thread;
+    return NKR_B200_OK;
+}
+
 int nkr_b200_set_autotune(nkr_b200_ctx *ctx, int enable)
 {
     NKR_REQUIRE(ctx, "null context");

@@ -1,4 +1,7 @@
 // Radix-2 NTT kernels and resident tables (see ntt.cuh for the design).
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include "ntt.cuh"
 
 namespace nkr {
@@ -179,27 +182,35 @@ __global__ void k_quotient(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_
     if (i < n) h[i] = (a[i] * b[i] - c[i]) * *zinv;
 }
 
-// pass split: at most 10 radix-2 stages per pass, spread evenly
-int pass_plan(int logn, int *ts)
+// pass split: at most max_stages radix-2 stages per pass, spread evenly
+// (ts holds up to 8 passes: max_stages >= 4 for logn <= 28)
+int pass_plan(int logn, int max_stages, int *ts)
 {
-    const int np = (logn + 9) / 10;
+    const int np = (logn + max_stages - 1) / max_stages;
     for (int i = 0; i < np; ++i) ts[i] = logn / np + (i < logn % np ? 1 : 0);
     return np;
+}
+
+unsigned pass_threads(int t, int bfly_per_thread)
+{
+    const unsigned half = 1u << (t - 1);
+    const unsigned th = half / unsigned(bfly_per_thread);
+    return (t >= 6 && th >= 32) ? th : 32u;
 }
 
 int run_passes(const NttTables &tb, Fr *data, bool dif, bool inverse, const Fr *pre,
                const Fr *post, const Fr *post_const, cudaStream_t st)
 {
     const int logn = tb.logn;
-    int ts[4];
-    const int np = pass_plan(logn, ts);
+    int ts[8];
+    const int np = pass_plan(logn, tb.max_stages, ts);
     const Fr *tw = inverse ? tb.tw_inv.as<Fr>() : tb.tw_fwd.as<Fr>();
     int s_lo = dif ? logn : 0;
     for (int p = 0; p < np; ++p) {
         const int t = ts[p];
         if (dif) s_lo -= t;
         const int G = 1 << t;
-        const unsigned threads = G >= 64 ? unsigned(G / 2) : 32u;
+        const unsigned threads = pass_threads(t, tb.bfly_per_thread);
         const unsigned blocks = unsigned(tb.n >> t);
         const Fr *pr = p == 0 ? pre : nullptr;
         const Fr *po = p == np - 1 ? post : nullptr;
@@ -212,6 +223,55 @@ int run_passes(const NttTables &tb, Fr *data, bool dif, bool inverse, const Fr *
         if (!dif) s_lo += t;
     }
     return NKR_B200_OK;
+}
+
+// NTT tile-shape autotuner: times a forward transform of the table's size for
+// every pass split with 7..10 stages per pass and 1, 2 or 4 butterflies per
+// thread and stage, and keeps the fastest (every shape gives the same output).
+// Sizes below 2^14 keep the default; NKR_B200_AUTOTUNE=0 turns it off.
+int ntt_tune(NttTables &t, Fr *work, cudaStream_t st)
+{
+    const char *e = std::getenv("NKR_B200_AUTOTUNE");
+    if (t.logn < 14 || (e && std::strcmp(e, "0") == 0)) return NKR_B200_OK;
+    cudaEvent_t e0, e1;
+    NKR_CUDA(cudaEventCreate(&e0));
+    NKR_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    int best_s = t.max_stages, best_b = t.bfly_per_thread;
+    int prev_ts[8] = {}, prev_np = 0;
+    int status = NKR_B200_OK;
+    for (int ms = 10; ms >= 7 && status == NKR_B200_OK; --ms) {
+        int ts[8];
+        const int np = pass_plan(t.logn, ms, ts);
+        if (np == prev_np && std::equal(ts, ts + np, prev_ts)) continue; // same split
+        std::copy(ts, ts + np, prev_ts);
+        prev_np = np;
+        for (int bpt = 1; bpt <= 4 && status == NKR_B200_OK; bpt *= 2) {
+            t.max_stages = ms;
+            t.bfly_per_thread = bpt;
+            status = run_passes(t, work, true, false, nullptr, nullptr, nullptr, st); // warm-up
+            if (status != NKR_B200_OK) break;
+            if (cudaEventRecord(e0, st) != cudaSuccess) status = NKR_B200_ECUDA;
+            for (int r = 0; r < 3 && status == NKR_B200_OK; ++r)
+                status = run_passes(t, work, true, false, nullptr, nullptr, nullptr, st);
+            float ms_run = 0.f;
+            if (status == NKR_B200_OK && (cudaEventRecord(e1, st) != cudaSuccess ||
+                                          cudaEventSynchronize(e1) != cudaSuccess ||
+                                          cudaEventElapsedTime(&ms_run, e0, e1) != cudaSuccess))
+                status = NKR_B200_ECUDA;
+            if (status == NKR_B200_OK && (best == 0.f || ms_run < best)) {
+                best = ms_run;
+                best_s = ms;
+                best_b = bpt;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t.max_stages = best_s;
+    t.bfly_per_thread = best_b;
+    if (status != NKR_B200_OK) set_error("NTT tile tuning failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return status;
 }
 
 } // namespace
@@ -254,6 +314,7 @@ int ntt_tables_build(NttTables &t, int logn, cudaStream_t st)
     k_bitrev_scaled<<<nb, 256, 0, st>>>(tmp.as<Fr>(), c + kConstNinv, t.t2.as<Fr>(), logn);
     NKR_CHECK_LAUNCH();
     NKR_CUDA(cudaStreamSynchronize(st));
+    NKR_TRY(ntt_tune(t, tmp.as<Fr>(), st));
     return NKR_B200_OK;
 }
 
@@ -321,14 +382,14 @@ int ntt_dit_raw(int logn, const Fr *tw, Fr *data, const Fr *pre, const Fr *post,
                 const Fr *post_const, cudaStream_t st)
 {
     NKR_REQUIRE(logn >= 1 && logn <= 28, "NTT domain 2^%d outside [2, 2^28]", logn);
-    int ts[4];
-    const int np = pass_plan(logn, ts);
+    int ts[8];
+    const int np = pass_plan(logn, 10, ts);
     const uint64_t n = uint64_t(1) << logn;
     int s_lo = 0;
     for (int p = 0; p < np; ++p) {
         const int t = ts[p];
         const int G = 1 << t;
-        const unsigned threads = G >= 64 ? unsigned(G / 2) : 32u;
+        const unsigned threads = pass_threads(t, 1);
         k_ntt_pass<false><<<unsigned(n >> t), threads, G * sizeof(Fr), st>>>(
             data, s_lo, t, tw, p == 0 ? pre : nullptr, p == np - 1 ? post : nullptr,
             p == np - 1 ? post_const : nullptr);

@@ -36,6 +36,11 @@ struct NttTables {
     DevBuf t1;      // Fr[N]: N^-1 g^bitrev(j)
     DevBuf t2;      // Fr[N]: N^-1 g^-bitrev(j)
     DevBuf consts;  // Fr[8]: w, w^-1, N^-1, (g^N - 1)^-1, g, g^-1
+    // tile shape of the passes, chosen on this device when the tables are built
+    // (ntt_tables_build): at most max_stages radix-2 stages per pass, each thread
+    // doing bfly_per_thread butterflies per stage
+    int max_stages = 10;
+    int bfly_per_thread = 1;
     size_t device_bytes() const
     {
         return tw_fwd.bytes + tw_inv.bytes + gpow.bytes + t1.bytes + t2.bytes + consts.bytes;

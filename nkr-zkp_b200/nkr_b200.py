@@ -92,6 +92,8 @@ _SIGS = {
     "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
                                             ctypes.POINTER(RawProofC)]),
     "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
+    "nkr_b200_tune_ntt": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)]),
     "nkr_b200_ntt_device": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, _U64, _VP,
                                            ctypes.POINTER(ctypes.c_float)]),
     "nkr_b200_server_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
@@ -279,6 +281,12 @@ class Context:
         _check(_lib.nkr_b200_ntt_device(self.h, op, in_ptr, out_ptr, n, stream_ptr,
                                         ctypes.byref(ms) if timed else None), f"ntt_device op {op}")
         return ms.value if timed else None
+
+    def tune_ntt(self, n):
+        """(max stages per pass, butterflies per thread) chosen for 2^k-point NTTs."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.nkr_b200_tune_ntt(self.h, n, ctypes.byref(a), ctypes.byref(b)), "tune_ntt")
+        return a.value, b.value
 
     def spmv(self, rows, cols, row_ptr, col_idx, values, z):
         y = np.zeros((rows, 4), np.uint64)

@@ -106,3 +106,18 @@ def test_device_entry_point_rejects_bad_buffers(ctx):
         ctx.ntt_device(0, host.ctypes.data, xd.data_ptr() + n * 32, n)
     with pytest.raises(nk.B200Error, match="power of two"):
         ctx.ntt_device(0, xd.data_ptr(), xd.data_ptr() + n * 32, 1000)
+
+
+@pytest.mark.parametrize("logn", [10, 16, 20])
+def test_tuned_tile_shape_is_in_range_and_exact(ctx, logn, rng):
+    """The NTT tile tuner picks a shape from its candidate set; the transforms
+    it drives stay bit-exact (inverse pairs are identities)."""
+    n = 1 << logn
+    stages, bpt = ctx.tune_ntt(n)
+    if logn < 14:
+        assert (stages, bpt) == (10, 1)
+    else:
+        assert 7 <= stages <= 10 and bpt in (1, 2, 4)
+    x = O.random_fr(n, rng)
+    assert np.array_equal(ctx.ntt(1, ctx.ntt(0, x)), x)
+    assert np.array_equal(ctx.ntt(3, ctx.ntt(2, x)), x)
