@@ -82,3 +82,34 @@ def test_rejects_unknown_key_and_request(ctx, keyset):
     with pytest.raises(nk.B200Error, match="unknown request"):
         sv.wait(12345)
     sv.close()
+
+
+def test_large_key_proves_one_request_at_a_time(ctx):
+    """A key of 2^19 rows fills the GPU alone: the server keeps it to one slot and
+    queues its other requests in arrival order, while a small key beside it
+    still takes several slots; every result equals the plain prove."""
+    big = nk.generate("matmul", 64, 0, seed=900)          # 266,240 rows -> 2^19
+    assert big.rows == 1 << 19
+    small = nk.generate("poseidon", 4, 1, seed=901)
+    bes = []
+    for r1, seed in ((big, 902), (small, 903)):
+        pk, _ = nk.setup(ctx, r1, O.random_fr(5, np.random.default_rng(seed)))
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        bes.append(be)
+    small_wits = [nk.generate("poseidon", 4, 1, seed=910 + i).witness for i in range(4)]
+    want_big = bytes(bes[0].prove(big.witness))
+    want_small = [bytes(bes[1].prove(w)) for w in small_wits]
+    sv = nk.Server(ctx, max_inflight=8, max_slots_per_key=4)
+    kb, ks = sv.add_key(bes[0]), sv.add_key(bes[1])
+    rb = [sv.submit(kb, big.witness) for _ in range(3)]
+    rs = [sv.submit(ks, w) for w in small_wits]
+    for r in rb:
+        assert bytes(sv.wait(r)[0]) == want_big
+    for r, w in zip(rs, want_small):
+        assert bytes(sv.wait(r)[0]) == w
+    assert sv.slots(kb) == 1
+    assert 1 <= sv.slots(ks) <= 4
+    sv.close()
+    for be in bes:
+        be.free()
