@@ -100,7 +100,7 @@ __device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
 } // namespace f52
 
 #ifdef NKR_FIELD_MUL_OUTLINE
-#define NKR_MUL52_ATTR __noinline__
+#define NKR_MUL52_ATTR inline __noinline__ // inline: one definition across translation units
 #else
 #define NKR_MUL52_ATTR __forceinline__
 #endif
@@ -215,6 +215,20 @@ __device__ NKR_MUL52_ATTR Fq52Pair mul52x2v(Fq52 a, Fq52 b, Fq52 c, Fq52 d)
     return r;
 }
 
+struct Fq52Triple {
+    Fq52 x, y, z;
+};
+
+// (a b, c d, e f) in one call: the three products of a Karatsuba Fq2 product
+__device__ NKR_MUL52_ATTR Fq52Triple mul52x3v(Fq52 a, Fq52 b, Fq52 c, Fq52 d, Fq52 e, Fq52 f)
+{
+    Fq52Triple r;
+    const Fq52 *pa[3] = {&a, &c, &e}, *pb[3] = {&b, &d, &f};
+    Fq52 *pr[3] = {&r.x, &r.y, &r.z};
+    mul52_body<3>(pa, pb, pr);
+    return r;
+}
+
 __device__ __forceinline__ void mul52x2(const Fq52 &a, const Fq52 &b, const Fq52 &c, const Fq52 &d,
                                         Fq52 &ab, Fq52 &cd)
 {
@@ -298,18 +312,39 @@ __device__ __forceinline__ Fq2x52 operator-(const Fq2x52 &a, const Fq2x52 &b)
 }
 __device__ __forceinline__ Fq2x52 neg(const Fq2x52 &a) { return {neg(a.c0), neg(a.c1)}; }
 __device__ __forceinline__ Fq2x52 dbl(const Fq2x52 &a) { return {dbl(a.c0), dbl(a.c1)}; }
+// Karatsuba, the three base-field products in one call (the FP64 Fq2 form serves
+// latency-bound single-thread chains, where one call of three interleaved
+// products takes far less than a pair and a single)
 __device__ __forceinline__ Fq2x52 operator*(const Fq2x52 &a, const Fq2x52 &b)
 {
-    Fq52 v0, v1;
-    mul52x2(a.c0, b.c0, a.c1, b.c1, v0, v1);
-    const Fq52 s = (a.c0 + a.c1) * (b.c0 + b.c1);
-    return {v0 - v1, s - v0 - v1};
+    const Fq52Triple t = mul52x3v(a.c0, b.c0, a.c1, b.c1, a.c0 + a.c1, b.c0 + b.c1);
+    return {t.x - t.y, t.z - t.x - t.y};
 }
 __device__ __forceinline__ Fq2x52 sqr(const Fq2x52 &a)
 {
     Fq52 p, q;
     mul52x2(a.c0 + a.c1, a.c0 - a.c1, a.c0, a.c1, p, q);
     return {p, q + q};
+}
+
+// Fermat inverse a^(p-2); R' products keep the R' domain.  0 maps to 0.
+__device__ inline Fq52 inverse(const Fq52 &a)
+{
+    const uint32_t e[8] = {FqParams::P0 - 2u, FqParams::P1, FqParams::P2, FqParams::P3,
+                           FqParams::P4,      FqParams::P5, FqParams::P6, FqParams::P7};
+    Fq52 acc = Fq52::one();
+    for (int i = 255; i >= 0; --i) {
+        acc = sqr(acc);
+        if ((e[i >> 5] >> (i & 31)) & 1) acc = acc * a;
+    }
+    return acc;
+}
+
+// 1 / (a0 + a1 u) = (a0 - a1 u) / (a0^2 + a1^2)
+__device__ inline Fq2x52 inverse(const Fq2x52 &a)
+{
+    const Fq52 ni = inverse(sqr(a.c0) + sqr(a.c1));
+    return {a.c0 * ni, neg(a.c1) * ni};
 }
 
 // ---------------------------------------------------------------------------

@@ -1,5 +1,5 @@
 // Groth16 prepare / prove / blind on one B200 (design notes in prover.cuh).
-// The blinding kernel chains scalar multiplications: out-of-line products.
+// Curve arithmetic in the finishing kernels: out-of-line products.
 #define NKR_FIELD_MUL_OUTLINE 1
 #include <algorithm>
 #include <cstring>
@@ -15,73 +15,6 @@ namespace {
 constexpr size_t kOutOffset[kNumMsm] = {0, 96, 192, 288, 384}; // A, B1, L, H, B2
 // issue order of the witness MSMs: the G2 MSM (longest) first
 constexpr int kWitnessOrder[4] = {kMsmB2, kMsmA, kMsmB1, kMsmL};
-
-// ---------------------------------------------------------------------------
-// blinding (protocol.cpp:85-94) with caller-supplied r, s
-// ---------------------------------------------------------------------------
-
-template <class F>
-__device__ __forceinline__ Affine<F> load_libff_affine(const F *p)
-{
-    if (p[2].is_zero()) return Affine<F>::inf();
-    return {p[0], p[1]};
-}
-
-template <class F>
-__device__ __forceinline__ void store_libff(const Xyzz<F> &x, F *out)
-{
-    const Affine<F> a = xyzz_to_affine(x);
-    if (a.is_inf()) {
-        out[0] = F::zero();
-        out[1] = F::one();
-        out[2] = F::zero();
-    } else {
-        out[0] = a.x;
-        out[1] = a.y;
-        out[2] = F::one();
-    }
-}
-
-// pk_const: alpha_g1, beta_g1, delta_g1 (G1Affine) then beta_g2, delta_g2 (G2Affine)
-// raw: libff layout ar, bs1, zk, qz (G1), bs2 (G2); rs: r, s (Montgomery)
-// out: A (G1, 96 B), B (G2, 192 B), C (G1, 96 B) in libff layout
-__global__ void k_blind(const uint8_t *pk_const, const uint8_t *raw, const Fr *rs, uint8_t *out)
-{
-    __shared__ G1Xyzz g1p[6];
-    __shared__ G2Xyzz g2p;
-    const G1Affine *g1c = reinterpret_cast<const G1Affine *>(pk_const);
-    const G2Affine *g2c = reinterpret_cast<const G2Affine *>(pk_const + 3 * sizeof(G1Affine));
-    const Fq *rq = reinterpret_cast<const Fq *>(raw);
-    const G1Affine ar = load_libff_affine(rq + 0), bs1 = load_libff_affine(rq + 3),
-                   zk = load_libff_affine(rq + 6), qz = load_libff_affine(rq + 9);
-    const G2Affine bs2 = load_libff_affine(reinterpret_cast<const Fq2 *>(raw + 384));
-    const Fr r = from_mont(rs[0]), s = from_mont(rs[1]), rsp = from_mont(rs[0] * rs[1]);
-    // independent scalar multiples, one per warp (lane 0) so they run concurrently
-    const int t = (threadIdx.x & 31) ? -1 : int(threadIdx.x >> 5);
-    if (t == 0) g1p[0] = xyzz_mul_canon(g1c[2], r.v);   // r delta1
-    if (t == 1) g1p[1] = xyzz_mul_canon(g1c[0], s.v);   // s alpha1
-    if (t == 2) g1p[2] = xyzz_mul_canon(g1c[1], r.v);   // r beta1
-    if (t == 3) g1p[3] = xyzz_mul_canon(g1c[2], rsp.v); // rs delta1
-    if (t == 4) g1p[4] = xyzz_mul_canon(ar, s.v);       // s ar
-    if (t == 5) g1p[5] = xyzz_mul_canon(bs1, r.v);      // r bs1
-    if (t == 6) g2p = xyzz_mul_canon(g2c[1], s.v);      // s delta2
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    // A = alpha1 + ar + r delta1
-    G1Xyzz A = xyzz_add_affine(xyzz_add_affine(g1p[0], g1c[0]), ar);
-    // B = beta2 + bs2 + s delta2
-    G2Xyzz B = xyzz_add_affine(xyzz_add_affine(g2p, g2c[0]), bs2);
-    // C = qz + zk + s A + r B1 - rs delta1
-    //   = qz + zk + s alpha1 + s ar + r beta1 + r bs1 + rs delta1
-    G1Xyzz C = xyzz_add_affine(xyzz_add_affine(g1p[1], qz), zk);
-    C = xyzz_add(C, g1p[4]);
-    C = xyzz_add(C, g1p[2]);
-    C = xyzz_add(C, g1p[5]);
-    C = xyzz_add(C, g1p[3]);
-    store_libff(A, reinterpret_cast<Fq *>(out));
-    store_libff(B, reinterpret_cast<Fq2 *>(out + 96));
-    store_libff(C, reinterpret_cast<Fq *>(out + 288));
-}
 
 } // namespace
 
@@ -201,12 +134,15 @@ int slot_add(nkr_b200_key *key)
     NKR_TRY(sl->cz.alloc(key->rows * 32, "cz"));
     NKR_TRY(sl->h.alloc(key->rows * 32, "H"));
     NKR_TRY(sl->out.alloc(kOutBytes, "proof points"));
-    bytes += sl->z.bytes + 4 * sl->az.bytes + sl->out.bytes;
+    // zeroed: the tables then describe the point at infinity until the first prove
+    NKR_TRY(sl->glv_tab.alloc(glv_tables_bytes(), "blinding GLV tables"));
+    NKR_CUDA(cudaMemset(sl->glv_tab.p, 0, sl->glv_tab.bytes));
+    bytes += sl->z.bytes + 4 * sl->az.bytes + sl->out.bytes + sl->glv_tab.bytes;
     for (int k = 0; k < 3; ++k) {
         NKR_TRY(sl->spmv_prod[k].alloc(std::max<uint64_t>(key->mat[k].nu, 1) * 32, "SpMV products"));
         bytes += sl->spmv_prod[k].bytes;
     }
-    if (cudaHostAlloc(&sl->pinned_out, kOutBytes + 384, cudaHostAllocDefault) != cudaSuccess) {
+    if (cudaHostAlloc(&sl->pinned_out, kOutBytes + kBlindStage, cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         set_error("pinned host allocation failed");
         return NKR_B200_ENOMEM;
@@ -244,6 +180,10 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed)
         NKR_TRY(msm_acc_run(key->bases[k], sl->sort_w[g], sl->acc[k], out + kOutOffset[k], sl->st[k]));
         NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
     }
+    // ar and bs1 tabulated for the blinding, behind the H chain on A's stream
+    NKR_CUDA(cudaStreamWaitEvent(sl->st[kMsmA], sl->ev_done[kMsmB1], 0));
+    NKR_TRY(glv_tables_issue(sl, sl->st[kMsmA]));
+    NKR_CUDA(cudaEventRecord(sl->ev_done[kMsmA], sl->st[kMsmA]));
     // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
     const NttTables &T = key->ntt;
     const Fr *cst = T.consts.as<Fr>();
@@ -403,7 +343,6 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
         }
         key->sort_of[k] = g;
     }
-    NKR_PREP(key->blind_io.alloc(64 + 384, "blinding io"));
     // PK constants: libff Jacobian -> affine
     {
         DevBuf stage;
@@ -427,6 +366,7 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
             return fail(NKR_B200_ECUDA);
         }
     }
+    NKR_PREP(blind_tables_build(key, st));
     NKR_PREP(slot_add(key));
 #undef NKR_PREP
     *out = key;
@@ -456,37 +396,6 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     NKR_CUDA(cudaEventElapsedTime(&key->times.total_ms, sl->ev_t[0], sl->ev_t[4]));
     key->times.witness_msms_ms = key->times.total_ms - ms[0];
     key->have_times = true;
-    return NKR_B200_OK;
-}
-
-int key_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r, const void *s,
-              nkr_b200_proof *res)
-{
-    NKR_REQUIRE(key && raw && r && s && res, "null argument");
-    NKR_CUDA(cudaSetDevice(key->ctx->device));
-    ProveSlot *sl = key->slots[0].get();
-    cudaStream_t s0 = sl->main();
-    uint8_t *host = static_cast<uint8_t *>(sl->pinned_out) + kOutBytes; // 384 B staging
-    uint8_t *dev = key->blind_io.as<uint8_t>();
-    // raw points go to the slot's out (device) in libff layout; r, s to blind_io[0, 64)
-    uint8_t staging[kOutBytes];
-    std::memcpy(staging + 0, raw->ar, 96);
-    std::memcpy(staging + 96, raw->bs1, 96);
-    std::memcpy(staging + 192, raw->zk, 96);
-    std::memcpy(staging + 288, raw->qz, 96);
-    std::memcpy(staging + 384, raw->bs2, 192);
-    NKR_CUDA(cudaStreamSynchronize(s0));
-    NKR_CUDA(cudaMemcpy(sl->out.p, staging, kOutBytes, cudaMemcpyHostToDevice));
-    NKR_CUDA(cudaMemcpy(dev, r, 32, cudaMemcpyHostToDevice));
-    NKR_CUDA(cudaMemcpy(dev + 32, s, 32, cudaMemcpyHostToDevice));
-    k_blind<<<1, 7 * 32, 0, s0>>>(key->pk_const.as<uint8_t>(), sl->out.as<uint8_t>(),
-                                  reinterpret_cast<const Fr *>(dev), dev + 64);
-    NKR_CHECK_LAUNCH();
-    NKR_CUDA(cudaMemcpyAsync(host, dev + 64, 384, cudaMemcpyDeviceToHost, s0));
-    NKR_CUDA(cudaStreamSynchronize(s0));
-    std::memcpy(res->a, host, 96);
-    std::memcpy(res->b, host + 96, 192);
-    std::memcpy(res->c, host + 288, 96);
     return NKR_B200_OK;
 }
 
@@ -615,7 +524,8 @@ void nkr_b200_key_free(nkr_b200_key *key)
 uint64_t nkr_b200_key_device_bytes(const nkr_b200_key *key)
 {
     if (!key) return 0;
-    uint64_t b = key->ntt.device_bytes() + key->pk_const.bytes + key->blind_io.bytes;
+    uint64_t b = key->ntt.device_bytes() + key->pk_const.bytes + key->blind_io.bytes +
+                 key->blind_tab.bytes;
     for (int k = 0; k < 3; ++k)
         b += key->mat[k].row_ptr.bytes + key->mat[k].col.bytes + key->mat[k].nu_col.bytes +
              key->mat[k].nu_val.bytes;

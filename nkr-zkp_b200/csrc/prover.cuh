@@ -48,6 +48,7 @@ namespace nkr {
 
 enum { kMsmA = 0, kMsmB1 = 1, kMsmL = 2, kMsmH = 3, kMsmB2 = 4, kNumMsm = 5 };
 constexpr size_t kOutBytes = 4 * 96 + 192; // ar, bs1, zk, qz (G1) + bs2 (G2), libff layout
+constexpr size_t kBlindStage = 1280;       // pinned staging of one blinding, after the results
 
 struct ProveSlot {
     MsmSort sort_w[4]; // witness digit sorts, one per distinct support
@@ -56,6 +57,7 @@ struct ProveSlot {
     DevBuf z, az, bz, cz, h;
     DevBuf spmv_prod[3]; // SpMV products of the non-unit terms, per matrix
     DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
+    DevBuf glv_tab; // ar and bs1 of the last prove, tabulated for blinding (blind.cu)
     cudaStream_t st[kNumMsm] = {};
     cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
@@ -67,7 +69,7 @@ struct ProveSlot {
     void *pinned_wit[2] = {nullptr, nullptr};
     cudaEvent_t ev_wit[2] = {nullptr, nullptr};
     int wit_next = 0;
-    void *pinned_out = nullptr; // kOutBytes + 384 (blinding)
+    void *pinned_out = nullptr; // kOutBytes + kBlindStage (blinding)
     cudaStream_t main() const { return st[kMsmH]; }
     ~ProveSlot();
 };
@@ -87,7 +89,8 @@ struct nkr_b200_key {
     int sort_of[nkr::kNumMsm] = {};
     int sort_stream[4] = {};
     nkr::DevBuf pk_const; // alpha_g1, beta_g1, delta_g1 (G1 affine) and beta_g2, delta_g2 (G2 affine)
-    nkr::DevBuf blind_io; // r, s in; proof out
+    nkr::DevBuf blind_io;  // raw proof and scalars in, proof out (blind.cu)
+    nkr::DevBuf blind_tab; // fixed-base tables of alpha1, beta1, delta1 (G1) and delta2 (G2)
     std::vector<std::unique_ptr<nkr::ProveSlot>> slots; // slots[0]: nkr_b200_prove
     uint64_t slot_bytes = 0;                            // device bytes of one slot
     nkr_b200_stage_times times{};
@@ -109,6 +112,13 @@ int slot_capture(nkr_b200_key *key, ProveSlot *slot);
 int slot_upload_witness(nkr_b200_key *key, ProveSlot *slot, const void *witness);
 // Replays the slot's graph on its main stream.
 int slot_launch(ProveSlot *slot);
+// Blinding buffers and the fixed-base tables of the key's alpha1, beta1, delta1
+// and delta2 (pk_const already resident); synchronises st.
+int blind_tables_build(nkr_b200_key *key, cudaStream_t st);
+// Device bytes of a slot's GLV tables, and their computation from the slot's
+// ar and bs1 (queued on st once both MSMs are final).
+size_t glv_tables_bytes();
+int glv_tables_issue(ProveSlot *slot, cudaStream_t st);
 // Affine-normalise the 4 G1 + 1 G2 result points (576 B, libff layout) in place.
 void normalize_raw(void *raw576);
 void raw_from_bytes(const void *raw576, nkr_b200_raw_proof *res);
