@@ -332,7 +332,9 @@ def run_b200(args):
         if i >= args.warmup:
             e2e.append((time.perf_counter() - t1) * 1e3)
     e2e_ms = replica_ms_per_proof(sum(e2e), len(e2e), world, dist, f"cuda:{device}")
-    h2d = r1.cols * 32 + 576 + 64
+    # witness; the blinding's upload: raw proof (576 B) + r, s as canonical scalars
+    # and their GLV halves (240 B); downloads: raw proof, then the proof (384 B)
+    h2d = r1.cols * 32 + 576 + 240
     d2h = 576 + 384
 
     # ---- roofline of the dominant kernel (MSM bucket accumulation) ---------------
