@@ -539,53 +539,6 @@ __global__ void k_jac_to_affine(const F *__restrict__ jac, Affine<F> *__restrict
     }
 }
 
-// XYZZ -> affine: 1/ZZ = t ZZZ, 1/ZZZ = t ZZ with t = 1/(ZZ ZZZ)
-template <class F>
-__global__ void k_xyzz_to_affine(const Xyzz<F> *__restrict__ in, Affine<F> *__restrict__ out,
-                                 uint64_t n)
-{
-    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t beg = t * kNormChunk;
-    if (beg >= n) return;
-    const int cnt = int(n - beg < uint64_t(kNormChunk) ? n - beg : uint64_t(kNormChunk));
-    F pre[kNormChunk];
-    F acc = F::one();
-    for (int j = 0; j < cnt; ++j) {
-        pre[j] = acc;
-        const Xyzz<F> p = in[beg + j];
-        if (!p.is_inf()) acc = acc * (p.zz * p.zzz);
-    }
-    F inv = inverse(acc);
-    for (int j = cnt - 1; j >= 0; --j) {
-        const Xyzz<F> p = in[beg + j];
-        if (p.is_inf()) {
-            out[beg + j] = Affine<F>::inf();
-            continue;
-        }
-        const F d = p.zz * p.zzz;
-        const F ti = inv * pre[j];
-        inv = inv * d;
-        out[beg + j] = {p.x * (ti * p.zzz), p.y * (ti * p.zz)};
-    }
-}
-
-// out[i] = 2^c * in[i]
-template <class F>
-__global__ void k_dbl_c(const Affine<F> *__restrict__ in, Xyzz<F> *__restrict__ out, uint64_t n,
-                        int c)
-{
-    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const Affine<F> p = in[i];
-    if (p.is_inf()) {
-        out[i] = Xyzz<F>::inf();
-        return;
-    }
-    Xyzz<F> x = xyzz_from_affine_dbl(p);
-    for (int d = 1; d < c; ++d) x = xyzz_dbl(x);
-    out[i] = x;
-}
-
 template <class P>
 __global__ void k_bitrev_points(const P *__restrict__ in, P *__restrict__ out, int logn)
 {
@@ -606,20 +559,87 @@ int jac_to_affine_t(const void *jac, void *aff, uint64_t n, cudaStream_t st)
     return NKR_B200_OK;
 }
 
+// Window copies k = 1..W-1 of the points [beg, beg + m): thread i runs the whole
+// doubling chain of point beg + i (c (W - 1) doublings, in the MSM's compute
+// field) and writes copy k to out[(k - 1) m + i] (XYZZ, storage domain).
+template <class F>
+__global__ void k_window_chain(const Affine<F> *__restrict__ pts, Xyzz<F> *__restrict__ out,
+                               uint64_t beg, uint64_t m, int c, int W)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    using C = CF<F>;
+    const Affine<F> s = pts[beg + i];
+    if (s.is_inf()) {
+        for (int k = 1; k < W; ++k) out[uint64_t(k - 1) * m + i] = Xyzz<F>::inf();
+        return;
+    }
+    const Affine<C> a = lda(s);
+    Xyzz<C> x = xyzz_from_affine_dbl(Affine<C>{msm_enter(a.x), msm_enter(a.y)});
+    for (int k = 1; k < W; ++k) {
+        for (int d = (k == 1 ? 1 : 0); d < c; ++d) x = xyzz_dbl(x);
+        out[uint64_t(k - 1) * m + i] = {msm_out(msm_leave(x.x)), msm_out(msm_leave(x.y)),
+                                        msm_out(msm_leave(x.zz)), msm_out(msm_leave(x.zzz))};
+    }
+}
+
+// XYZZ copies of k_window_chain -> affine copies k = 1..W-1 in the bases
+// (copy k of point beg + i at pts[k n + beg + i]); batch inversion per chunk of
+// kNormChunk scratch entries (a chunk may span two copies: the mapping is per entry)
+template <class F>
+__global__ void k_window_affine(const Xyzz<F> *__restrict__ in, Affine<F> *__restrict__ pts,
+                                uint64_t n, uint64_t beg, uint64_t m, uint64_t count)
+{
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t first = t * kNormChunk;
+    if (first >= count) return;
+    const int cnt = int(count - first < uint64_t(kNormChunk) ? count - first : uint64_t(kNormChunk));
+    F pre[kNormChunk];
+    F acc = F::one();
+    for (int j = 0; j < cnt; ++j) {
+        pre[j] = acc;
+        const Xyzz<F> p = in[first + j];
+        if (!p.is_inf()) acc = acc * (p.zz * p.zzz);
+    }
+    F inv = inverse(acc);
+    for (int j = cnt - 1; j >= 0; --j) {
+        const uint64_t e = first + j;
+        const uint64_t dst = (e / m + 1) * n + beg + e % m;
+        const Xyzz<F> p = in[e];
+        if (p.is_inf()) {
+            pts[dst] = Affine<F>::inf();
+            continue;
+        }
+        const F d = p.zz * p.zzz;
+        const F ti = inv * pre[j];
+        inv = inv * d;
+        pts[dst] = {p.x * (ti * p.zzz), p.y * (ti * p.zz)};
+    }
+}
+
+// The W - 1 folded window copies 2^(c k) P of every base: per chunk of points one
+// launch runs every copy's doublings (so a small key pays one doubling chain and
+// one batch inversion, not W - 1 of each) and one launch converts them to affine.
 template <class F>
 int build_windows_t(MsmBases &b, cudaStream_t st)
 {
     const MsmShape &sh = b.shape;
+    if (sh.W < 2 || sh.n == 0) return NKR_B200_OK;
     Affine<F> *pts = b.pts.as<Affine<F>>();
+    const uint64_t copies = uint64_t(sh.W - 1);
+    // scratch of at most ~1 GiB: chunk * copies XYZZ points
+    const uint64_t cap = std::max<uint64_t>(1, (uint64_t(1) << 30) / (copies * sizeof(Xyzz<F>)));
+    const uint64_t chunk = std::min<uint64_t>(sh.n, cap);
     DevBuf tmp;
-    NKR_TRY(tmp.alloc(sh.n * sizeof(Xyzz<F>), "window copy scratch"));
-    const uint64_t chunks = (sh.n + kNormChunk - 1) / kNormChunk;
-    for (int k = 1; k < sh.W; ++k) {
-        k_dbl_c<F><<<blocks_for(sh.n, 128), 128, 0, st>>>(pts + uint64_t(k - 1) * sh.n,
-                                                          tmp.as<Xyzz<F>>(), sh.n, sh.c);
+    NKR_TRY(tmp.alloc(chunk * copies * sizeof(Xyzz<F>), "window copy scratch"));
+    for (uint64_t beg = 0; beg < sh.n; beg += chunk) {
+        const uint64_t m = std::min<uint64_t>(chunk, sh.n - beg);
+        k_window_chain<F><<<blocks_for(m, 128), 128, 0, st>>>(pts, tmp.as<Xyzz<F>>(), beg, m, sh.c,
+                                                              sh.W);
         NKR_CHECK_LAUNCH();
-        k_xyzz_to_affine<F><<<blocks_for(chunks, 64), 64, 0, st>>>(tmp.as<Xyzz<F>>(),
-                                                                   pts + uint64_t(k) * sh.n, sh.n);
+        const uint64_t count = m * copies;
+        k_window_affine<F><<<blocks_for((count + kNormChunk - 1) / kNormChunk, 64), 64, 0, st>>>(
+            tmp.as<Xyzz<F>>(), pts, sh.n, beg, m, count);
         NKR_CHECK_LAUNCH();
     }
     NKR_CUDA(cudaStreamSynchronize(st));

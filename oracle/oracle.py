@@ -424,6 +424,7 @@ class RefCuda:
         self.lib.refcuda_open.argtypes = [_VP] + [_VP] * 5
         self.lib.refcuda_prove.argtypes = [_VP, _VP, _VP, _VP, ctypes.POINTER(ctypes.c_double)]
         self.lib.refcuda_close.argtypes = [_VP]
+        self.lib.refcuda_last_prepare_ms.restype = ctypes.c_double
 
     def open(self, r1cs, pk):
         c = Oracle._circuit(None, r1cs)
@@ -441,6 +442,10 @@ class RefCuda:
         if self.lib.refcuda_prove(h, _p(_arr(witness)), _p(g1), _p(g2), ctypes.byref(ms)) != 0:
             raise RuntimeError(self.lib.refcuda_last_error().decode())
         return g1.reshape(4, 8), g2, ms.value
+
+    def last_prepare_ms(self):
+        """host wall ms of the last open's CudaBackend::prepare (synchronised)"""
+        return self.lib.refcuda_last_prepare_ms()
 
     def close(self, h):
         self.lib.refcuda_close(h)

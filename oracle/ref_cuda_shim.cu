@@ -10,6 +10,7 @@
 // copies only (X, Y) of each proving-key point (operators/cuda/include/msm/
 // msm.cuh:51-57), so the keys handed in must be affine-normalised (Z = 1).
 #include <chrono>
+#include <cuda_runtime.h>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -39,6 +40,7 @@ struct RawCircuit {
 namespace {
 
 thread_local std::string g_error;
+thread_local double g_prepare_ms = 0;
 
 template <typename T>
 std::vector<T> from_raw(const void *p, std::size_t n)
@@ -75,6 +77,10 @@ extern "C" {
 
 const char *refcuda_last_error(void) { return g_error.c_str(); }
 
+// Host wall time of the last refcuda_open's CudaBackend::prepare (device
+// layout, key upload), followed by a device synchronisation.
+double refcuda_last_prepare_ms(void) { return g_prepare_ms; }
+
 // Builds the circuit and proving key from raw buffers and runs the reference's
 // CudaBackend::prepare (device layout, key upload).  Queries: a, b_g1, l (G1[cols]),
 // b_g2 (G2[cols]), h (G1[rows]) in libff Jacobian layout with Z = 1.
@@ -101,7 +107,11 @@ void *refcuda_open(const RawCircuit *rc, const void *a_query, const void *b_g1_q
         p->pk.alpha_g1 = p->pk.beta_g1 = p->pk.delta_g1 = G1::one();
         p->pk.beta_g2 = p->pk.delta_g2 = G2::one();
         p->backend = make_cuda_backend();
+        const auto t0 = std::chrono::steady_clock::now();
         p->backend->prepare(p->circuit, p->pk);
+        cudaDeviceSynchronize();
+        const auto t1 = std::chrono::steady_clock::now();
+        g_prepare_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
         return p.release();
     } catch (const std::exception &e) {
         g_error = e.what();
