@@ -133,7 +133,11 @@ int nkr_b200_prove(nkr_b200_key *key, const void *witness, uint64_t n,
                    nkr_b200_raw_proof *out);
 
 /* Replaces blind_proof (common/src/protocol.cpp:85-94) with caller-given r, s
- * (Fr Montgomery, 32 B each); the reference draws them unseeded (:87-88). */
+ * (Fr Montgomery, 32 B each); the reference draws them unseeded (:87-88).
+ * raw: libff Jacobian points with any Z (as the reference's RawProof allows).
+ * The blinding of the last proof of this key's nkr_b200_prove reads tables that
+ * prove left on the device; any other raw proof gives the same result by a
+ * slower path (about 1 ms).  out: affine-normalised (Z = 1, or (0, 1, 0)). */
 int nkr_b200_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r,
                    const void *s, nkr_b200_proof *out);
 
