@@ -14,10 +14,10 @@
 //  - the two multiples of proof points (s ar, r bs1) use the GLV endomorphism of
 //    BN254 G1 (Gallant, Lambert and Vanstone, CRYPTO 2001): k = k1 + k2 lambda
 //    (mod r) with |k1|, |k2| < 2^127, and k P = k1 P + k2 phi(P) with
-//    phi(x, y) = (beta x, y).  Every prove ends by tabulating d 2^(8j) P
-//    (j < 16, d < 256) for its own ar and bs1 on a side stream, behind the H
-//    MSM (glv_tables_issue); when the raw proof handed to the blinding is the
-//    last proof of slot 0, one warp per point then looks up the 32 digits of
+//    phi(x, y) = (beta x, y).  A prove through nkr_b200_prove (slot 0) ends by
+//    tabulating d 2^(8j) P (j < 16, d < 256) for its own ar and bs1 on a side
+//    stream, behind the H MSM (glv_tables_issue); when the raw proof handed to
+//    the blinding is that proof, one warp per point looks up the 32 digits of
 //    k1 and k2 and sums them like the fixed bases.  Any other raw proof takes
 //    the chain: the two 127-bit halves run as 4-bit window chains on two lanes
 //    of the point's warp, from a 16-entry table its lanes build in parallel;

@@ -134,9 +134,12 @@ int slot_add(nkr_b200_key *key)
     NKR_TRY(sl->cz.alloc(key->rows * 32, "cz"));
     NKR_TRY(sl->h.alloc(key->rows * 32, "H"));
     NKR_TRY(sl->out.alloc(kOutBytes, "proof points"));
-    // zeroed: the tables then describe the point at infinity until the first prove
-    NKR_TRY(sl->glv_tab.alloc(glv_tables_bytes(), "blinding GLV tables"));
-    NKR_CUDA(cudaMemset(sl->glv_tab.p, 0, sl->glv_tab.bytes));
+    // slot 0 (nkr_b200_prove) keeps the GLV tables of its last proof for the
+    // blinding; zeroed, they describe the point at infinity until the first prove
+    if (key->slots.empty()) {
+        NKR_TRY(sl->glv_tab.alloc(glv_tables_bytes(), "blinding GLV tables"));
+        NKR_CUDA(cudaMemset(sl->glv_tab.p, 0, sl->glv_tab.bytes));
+    }
     bytes += sl->z.bytes + 4 * sl->az.bytes + sl->out.bytes + sl->glv_tab.bytes;
     for (int k = 0; k < 3; ++k) {
         NKR_TRY(sl->spmv_prod[k].alloc(std::max<uint64_t>(key->mat[k].nu, 1) * 32, "SpMV products"));
@@ -152,7 +155,7 @@ int slot_add(nkr_b200_key *key)
     return NKR_B200_OK;
 }
 
-int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed)
+int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
 {
     cudaStream_t s0 = sl->main();
     const uint64_t rows = key->rows;
@@ -181,9 +184,11 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed)
         NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
     }
     // ar and bs1 tabulated for the blinding, behind the H chain on A's stream
-    NKR_CUDA(cudaStreamWaitEvent(sl->st[kMsmA], sl->ev_done[kMsmB1], 0));
-    NKR_TRY(glv_tables_issue(sl, sl->st[kMsmA]));
-    NKR_CUDA(cudaEventRecord(sl->ev_done[kMsmA], sl->st[kMsmA]));
+    if (blind_tables) {
+        NKR_CUDA(cudaStreamWaitEvent(sl->st[kMsmA], sl->ev_done[kMsmB1], 0));
+        NKR_TRY(glv_tables_issue(sl, sl->st[kMsmA]));
+        NKR_CUDA(cudaEventRecord(sl->ev_done[kMsmA], sl->st[kMsmA]));
+    }
     // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
     const NttTables &T = key->ntt;
     const Fr *cst = T.consts.as<Fr>();
@@ -210,7 +215,7 @@ int slot_capture(nkr_b200_key *key, ProveSlot *sl)
     cudaStream_t s0 = sl->main();
     const unsigned long long before = g_kernel_launches.load();
     NKR_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
-    const int s = prove_issue(key, sl, false);
+    const int s = prove_issue(key, sl, false, false);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(s0, &g);
     // capturing records kernels, it launches none
@@ -383,7 +388,7 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     cudaStream_t s0 = sl->main();
     // s0 is ordered after the previous prove's joins, so z is free to overwrite
     NKR_CUDA(cudaMemcpyAsync(sl->z.p, witness, n * 32, copy_kind_from(witness), s0));
-    NKR_TRY(prove_issue(key, sl, true));
+    NKR_TRY(prove_issue(key, sl, true, true));
     NKR_CUDA(cudaMemcpyAsync(sl->pinned_out, sl->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
     NKR_CUDA(cudaStreamSynchronize(s0));
     normalize_raw(sl->pinned_out);

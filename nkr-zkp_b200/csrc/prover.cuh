@@ -57,7 +57,7 @@ struct ProveSlot {
     DevBuf z, az, bz, cz, h;
     DevBuf spmv_prod[3]; // SpMV products of the non-unit terms, per matrix
     DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
-    DevBuf glv_tab; // ar and bs1 of the last prove, tabulated for blinding (blind.cu)
+    DevBuf glv_tab; // slot 0: ar and bs1 of its last prove, tabulated for blinding (blind.cu)
     cudaStream_t st[kNumMsm] = {};
     cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
@@ -103,8 +103,11 @@ namespace nkr {
 int slot_add(nkr_b200_key *key);
 // Issue one full prove on a slot's streams, witness already in slot->z.
 // Results land in slot->out (device, Jacobian with arbitrary Z).  No host
-// synchronisation; with timed, events bracket the stages on the main stream.
-int prove_issue(nkr_b200_key *key, ProveSlot *slot, bool timed);
+// synchronisation; with timed, events bracket the stages on the main stream;
+// with blind_tables (slot 0, nkr_b200_prove) the slot's GLV tables of ar and bs1
+// are computed for a following blinding (the captured graphs of batches and the
+// server leave them out).
+int prove_issue(nkr_b200_key *key, ProveSlot *slot, bool timed, bool blind_tables);
 // Captures prove_issue into the slot's graph (once).
 int slot_capture(nkr_b200_key *key, ProveSlot *slot);
 // Queues the witness upload (device, pinned or pageable host memory) on the
