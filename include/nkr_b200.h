@@ -44,6 +44,7 @@ enum {
 
 typedef struct nkr_b200_ctx nkr_b200_ctx;   /* one GPU: streams, scratch arena */
 typedef struct nkr_b200_key nkr_b200_key;   /* a prepared (circuit, proving key) */
+typedef struct nkr_b200_vk nkr_b200_vk;     /* a prepared verification key */
 typedef struct nkr_b200_msm_bases nkr_b200_msm_bases; /* resident MSM bases */
 
 /* Circuit in the reference's CSR layout: matrices A, B, C share the shape
@@ -81,6 +82,17 @@ typedef struct {
     uint8_t b[192];
     uint8_t c[96];
 } nkr_b200_proof;
+
+/* VerificationKey (types.hpp:40-45) in libff layout: e(alpha, beta) as
+ * alt_bn128_Fq12 (384 B), gamma and delta as G2 (192 B, any Z), ic as n_ic G1
+ * points (96 B each, any Z). */
+typedef struct {
+    const void *alpha_g1_beta_g2;
+    const void *gamma_g2;
+    const void *delta_g2;
+    const void *ic;
+    uint64_t n_ic;
+} nkr_b200_verification_key;
 
 /* Per-stage device times of the last prove on a key, milliseconds (CUDA events):
  * the reference's profile labels groth16.cuda.prove.{r1cs_matrix_vector,
@@ -140,6 +152,31 @@ int nkr_b200_prove(nkr_b200_key *key, const void *witness, uint64_t n,
  * slower path (about 1 ms).  out: affine-normalised (Z = 1, or (0, 1, 0)). */
 int nkr_b200_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void *r,
                    const void *s, nkr_b200_proof *out);
+
+/* ---- verification -------------------------------------------------------- */
+
+/* Prepares a verification key on the device (ic normalised, the Miller-loop
+ * lines of gamma and delta computed once). */
+int nkr_b200_vk_prepare(nkr_b200_ctx *ctx, const nkr_b200_verification_key *vk,
+                        nkr_b200_vk **out);
+
+/* Replaces verify (common/src/protocol.cpp:96-108) for a batch of count proofs
+ * of one key, one proof per GPU thread.  proofs: count nkr_b200_proof records
+ * (A, B, C in libff layout, any Z) in host memory; public_inputs: count rows of
+ * n_public Fr (Montgomery, 32 B each).  accept[i] = 1 when proof i satisfies
+ * e(A, B) = e(alpha, beta) e(vk_x, gamma) e(C, delta), else 0; as in the
+ * reference, every proof is rejected when n_public + 1 != n_ic.  The GT values
+ * are libff's (its reduced pairing, bit for bit), so the verdicts are the
+ * reference's. */
+int nkr_b200_verify_batch(nkr_b200_vk *vk, const void *public_inputs, uint64_t n_public,
+                          const void *proofs, uint64_t count, uint8_t *accept);
+void nkr_b200_vk_free(nkr_b200_vk *vk);
+
+/* Replaces Curve::reduced_pairing (libff alt_bn128_reduced_pairing) for count
+ * pairs: p_g1 G1[count] (96 B), q_g2 G2[count] (192 B), out_gt Fq12[count]
+ * (384 B, libff alt_bn128_Fq12 layout, Montgomery). */
+int nkr_b200_reduced_pairing(nkr_b200_ctx *ctx, const void *p_g1, const void *q_g2,
+                             uint64_t count, void *out_gt);
 
 /* Intermediates of the last prove on this key, copied to host (for parity
  * checks): az, bz, cz (Fr[rows]) and H (Fr[rows]); any pointer may be NULL. */

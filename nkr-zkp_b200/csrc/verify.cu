@@ -1,0 +1,229 @@
+// Groth16 verification on one B200: the reference's verify
+// (protocols/groth16/common/src/protocol.cpp:96-108) for a batch of proofs of
+// one verification key, one proof per thread, and the reduced pairing as an
+// operator (libff Curve::reduced_pairing).
+//
+// The reference checks e(A, B) == e(alpha, beta) e(vk_x, gamma) e(C, delta)
+// with three reduced pairings, vk_x = ic[0] + sum_j x_j ic[j + 1].  Here each
+// thread runs one Miller loop over the three pairs (A, B), (-vk_x, gamma),
+// (-C, delta) and one final exponentiation, and compares with the key's
+// e(alpha, beta): the same equation in GT, since the final exponentiation is a
+// homomorphism.  gamma and delta are fixed per key, so their Miller-loop lines
+// are computed once when the key is prepared; per proof only B's lines are
+// computed (affine, one Fq2 inversion per line).
+#define NKR_FIELD_MUL_OUTLINE 1
+#include <cstring>
+
+#include "pairing.cuh"
+#include "prover.cuh"
+
+struct nkr_b200_vk {
+    nkr_b200_ctx *ctx = nullptr;
+    uint64_t n_ic = 0;
+    nkr::DevBuf gt;    // e(alpha, beta): libff alt_bn128_Fq12, 384 B
+    nkr::DevBuf ic;    // ic[] as G1 affine (R domain)
+    nkr::DevBuf lines; // kAteLines lines of gamma, then of delta
+    nkr::DevBuf flags; // int[2]: gamma, delta at infinity
+    nkr::DevBuf io;    // batch staging (grown on demand)
+};
+
+namespace nkr {
+
+namespace {
+
+constexpr size_t kProofBytes = 96 + 192 + 96; // A, B, C in libff layout
+
+// libff Jacobian (X, Y, Z) -> affine; Z = 0 is infinity
+template <class F>
+__device__ __forceinline__ Affine<F> libff_to_affine(const F *p)
+{
+    if (p[2].is_zero()) return Affine<F>::inf();
+    const F zi = inverse(p[2]);
+    const F zi2 = sqr(zi);
+    return {p[0] * zi2, p[1] * (zi2 * zi)};
+}
+
+__device__ __forceinline__ Affine<Fq> g1_neg(const Affine<Fq> &p) { return affine_neg(p); }
+
+// gamma (lane 0) and delta (lane 1): Miller-loop lines; lanes also normalise ic
+__global__ void __launch_bounds__(32) k_vk_setup(const Fq2 *gd_jac, const Fq *ic_jac, uint64_t n_ic,
+                                                 AteLine *lines, int *flags, G1Affine *ic_aff)
+{
+    const int lane = threadIdx.x;
+    for (uint64_t i = lane; i < n_ic; i += 32) ic_aff[i] = libff_to_affine(ic_jac + 3 * i);
+    if (lane < 2) {
+        const Affine<Fq2> q = libff_to_affine(gd_jac + 3 * lane);
+        flags[lane] = q.is_inf() ? 1 : 0;
+        if (!q.is_inf()) ate_lines(q, lines + lane * kAteLines);
+    }
+}
+
+// reduced pairings of count (P, Q) pairs, one per thread
+__global__ void __launch_bounds__(64) k_pairing(const Fq *p_jac, const Fq2 *q_jac, uint64_t count,
+                                                Fq12 *out)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const Affine<Fq> p = libff_to_affine(p_jac + 3 * i);
+    const Affine<Fq2> q = libff_to_affine(q_jac + 3 * i);
+    if (p.is_inf() || q.is_inf()) {
+        out[i] = fq12_one();
+        return;
+    }
+    Fq12 f = fq12_one();
+    Affine<Fq2> t = q;
+    for (int b = kAteTopBit - 1; b >= 0; --b) {
+        f = sqr(f);
+        f = apply_line(f, ate_double(t), p);
+        if (ate_bit(b)) f = apply_line(f, ate_add(t, q), p);
+    }
+    f = apply_line(f, ate_add(t, twist_frobenius(q)), p);
+    f = apply_line(f, ate_add(t, twist_neg_frobenius2(q)), p);
+    out[i] = final_exponentiation(f);
+}
+
+// One proof per thread: proofs[i] = A (G1), B (G2), C (G1) in libff layout;
+// publics[i * n_pub + j] = x_j (Fr, Montgomery).
+__global__ void __launch_bounds__(64) k_verify(const Fq12 *gt, const G1Affine *ic, uint64_t n_ic,
+                                               const AteLine *lines, const int *flags,
+                                               const uint8_t *proofs, const Fr *publics,
+                                               uint64_t count, uint8_t *accept)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint8_t *pr = proofs + i * kProofBytes;
+    const Affine<Fq> a = libff_to_affine(reinterpret_cast<const Fq *>(pr));
+    const Affine<Fq2> b = libff_to_affine(reinterpret_cast<const Fq2 *>(pr + 96));
+    const Affine<Fq> c = libff_to_affine(reinterpret_cast<const Fq *>(pr + 288));
+    // vk_x = ic[0] + sum_j x_j ic[j + 1]
+    G1Xyzz acc = ic[0].is_inf() ? G1Xyzz::inf() : G1Xyzz{ic[0].x, ic[0].y, Fq::one(), Fq::one()};
+    const uint64_t n_pub = n_ic - 1;
+    for (uint64_t j = 0; j < n_pub; ++j) {
+        const Fr x = from_mont(publics[i * n_pub + j]);
+        acc = xyzz_add(acc, xyzz_mul_canon(ic[j + 1], x.v));
+    }
+    const Affine<Fq> nvk = g1_neg(xyzz_to_affine(acc));
+    const Affine<Fq> nc = g1_neg(c);
+    const bool on1 = !a.is_inf() && !b.is_inf();
+    const bool on2 = !nvk.is_inf() && !flags[0];
+    const bool on3 = !nc.is_inf() && !flags[1];
+    const AteLine *lg = lines, *ld = lines + kAteLines;
+    Fq12 f = fq12_one();
+    Affine<Fq2> t = b;
+    int s = 0;
+    for (int bit = kAteTopBit - 1; bit >= 0; --bit) {
+        f = sqr(f);
+        if (on1) f = apply_line(f, ate_double(t), a);
+        if (on2) f = apply_line(f, lg[s], nvk);
+        if (on3) f = apply_line(f, ld[s], nc);
+        ++s;
+        if (ate_bit(bit)) {
+            if (on1) f = apply_line(f, ate_add(t, b), a);
+            if (on2) f = apply_line(f, lg[s], nvk);
+            if (on3) f = apply_line(f, ld[s], nc);
+            ++s;
+        }
+    }
+    for (int k = 0; k < 2; ++k, ++s) {
+        if (on1) f = apply_line(f, ate_add(t, k == 0 ? twist_frobenius(b) : twist_neg_frobenius2(b)), a);
+        if (on2) f = apply_line(f, lg[s], nvk);
+        if (on3) f = apply_line(f, ld[s], nc);
+    }
+    accept[i] = final_exponentiation(f) == gt[0] ? 1 : 0;
+}
+
+} // namespace
+
+} // namespace nkr
+
+using namespace nkr;
+
+extern "C" {
+
+int nkr_b200_vk_prepare(nkr_b200_ctx *ctx, const nkr_b200_verification_key *vk, nkr_b200_vk **out)
+{
+    NKR_REQUIRE(ctx && vk && out, "null argument");
+    NKR_REQUIRE(vk->alpha_g1_beta_g2 && vk->gamma_g2 && vk->delta_g2 && vk->ic && vk->n_ic >= 1,
+                "verification key: every part is required and ic holds at least one point");
+    NKR_CUDA(cudaSetDevice(ctx->device));
+    auto key = std::make_unique<nkr_b200_vk>();
+    key->ctx = ctx;
+    key->n_ic = vk->n_ic;
+    cudaStream_t st = ctx->stream;
+    DevBuf stage;
+    NKR_TRY(stage.alloc(2 * 192 + vk->n_ic * 96, "verification key upload"));
+    uint8_t *sp = stage.as<uint8_t>();
+    NKR_CUDA(cudaMemcpyAsync(sp, vk->gamma_g2, 192, cudaMemcpyHostToDevice, st));
+    NKR_CUDA(cudaMemcpyAsync(sp + 192, vk->delta_g2, 192, cudaMemcpyHostToDevice, st));
+    NKR_CUDA(cudaMemcpyAsync(sp + 384, vk->ic, vk->n_ic * 96, cudaMemcpyHostToDevice, st));
+    NKR_TRY(key->gt.alloc(sizeof(Fq12), "e(alpha, beta)"));
+    NKR_CUDA(cudaMemcpyAsync(key->gt.p, vk->alpha_g1_beta_g2, sizeof(Fq12), cudaMemcpyHostToDevice, st));
+    NKR_TRY(key->ic.alloc(vk->n_ic * sizeof(G1Affine), "ic"));
+    NKR_TRY(key->lines.alloc(2 * kAteLines * sizeof(AteLine), "gamma / delta lines"));
+    NKR_TRY(key->flags.alloc(2 * sizeof(int), "gamma / delta flags"));
+    k_vk_setup<<<1, 32, 0, st>>>(reinterpret_cast<const Fq2 *>(sp), reinterpret_cast<const Fq *>(sp + 384),
+                                 vk->n_ic, key->lines.as<AteLine>(), key->flags.as<int>(),
+                                 key->ic.as<G1Affine>());
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaStreamSynchronize(st));
+    *out = key.release();
+    return NKR_B200_OK;
+}
+
+int nkr_b200_verify_batch(nkr_b200_vk *vk, const void *public_inputs, uint64_t n_public,
+                          const void *proofs, uint64_t count, uint8_t *accept)
+{
+    NKR_REQUIRE(vk && accept && (count == 0 || proofs), "null argument");
+    NKR_REQUIRE(n_public == 0 || count == 0 || public_inputs, "null public inputs");
+    if (count == 0) return NKR_B200_OK;
+    // the reference rejects a proof whose public input count does not match ic
+    if (n_public + 1 != vk->n_ic) {
+        std::memset(accept, 0, count);
+        return NKR_B200_OK;
+    }
+    NKR_CUDA(cudaSetDevice(vk->ctx->device));
+    cudaStream_t st = vk->ctx->stream;
+    const uint64_t pb = count * kProofBytes, xb = count * n_public * 32;
+    NKR_TRY(vk->io.alloc(pb + xb + count, "verification batch"));
+    uint8_t *dp = vk->io.as<uint8_t>();
+    NKR_CUDA(cudaMemcpyAsync(dp, proofs, pb, cudaMemcpyHostToDevice, st));
+    if (xb) NKR_CUDA(cudaMemcpyAsync(dp + pb, public_inputs, xb, cudaMemcpyHostToDevice, st));
+    k_verify<<<blocks_for(count, 64), 64, 0, st>>>(vk->gt.as<Fq12>(), vk->ic.as<G1Affine>(), vk->n_ic,
+                                                   vk->lines.as<AteLine>(), vk->flags.as<int>(), dp,
+                                                   reinterpret_cast<const Fr *>(dp + pb), count,
+                                                   dp + pb + xb);
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaMemcpyAsync(accept, dp + pb + xb, count, cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+void nkr_b200_vk_free(nkr_b200_vk *vk)
+{
+    if (!vk) return;
+    cudaSetDevice(vk->ctx->device);
+    delete vk;
+}
+
+int nkr_b200_reduced_pairing(nkr_b200_ctx *ctx, const void *p_g1, const void *q_g2, uint64_t count,
+                             void *out_gt)
+{
+    NKR_REQUIRE(ctx && (count == 0 || (p_g1 && q_g2 && out_gt)), "null argument");
+    if (count == 0) return NKR_B200_OK;
+    NKR_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    DevBuf buf;
+    NKR_TRY(buf.alloc(count * (96 + 192 + sizeof(Fq12)), "pairing buffers"));
+    uint8_t *b = buf.as<uint8_t>();
+    NKR_CUDA(cudaMemcpyAsync(b, p_g1, count * 96, cudaMemcpyHostToDevice, st));
+    NKR_CUDA(cudaMemcpyAsync(b + count * 96, q_g2, count * 192, cudaMemcpyHostToDevice, st));
+    Fq12 *o = reinterpret_cast<Fq12 *>(b + count * 288);
+    k_pairing<<<blocks_for(count, 64), 64, 0, st>>>(reinterpret_cast<const Fq *>(b),
+                                                    reinterpret_cast<const Fq2 *>(b + count * 96), count, o);
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaMemcpyAsync(out_gt, o, count * sizeof(Fq12), cudaMemcpyDeviceToHost, st));
+    NKR_CUDA(cudaStreamSynchronize(st));
+    return NKR_B200_OK;
+}
+
+} // extern "C"

@@ -56,6 +56,11 @@ class ProofC(ctypes.Structure):
     _fields_ = [("a", ctypes.c_uint8 * 96), ("b", ctypes.c_uint8 * 192), ("c", ctypes.c_uint8 * 96)]
 
 
+class VerificationKeyC(ctypes.Structure):
+    _fields_ = [("alpha_g1_beta_g2", _VP), ("gamma_g2", _VP), ("delta_g2", _VP), ("ic", _VP),
+                ("n_ic", _U64)]
+
+
 class StageTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in
                 ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms")]
@@ -85,6 +90,11 @@ _SIGS = {
     "nkr_b200_key_free": (None, [_VP]),
     "nkr_b200_key_device_bytes": (_U64, [_VP]),
     "nkr_b200_prove": (ctypes.c_int, [_VP, _VP, _U64, ctypes.POINTER(RawProofC)]),
+    "nkr_b200_vk_prepare": (ctypes.c_int, [_VP, ctypes.POINTER(VerificationKeyC),
+                                           ctypes.POINTER(_VP)]),
+    "nkr_b200_verify_batch": (ctypes.c_int, [_VP, _VP, _U64, _VP, _U64, _VP]),
+    "nkr_b200_vk_free": (None, [_VP]),
+    "nkr_b200_reduced_pairing": (ctypes.c_int, [_VP, _VP, _VP, _U64, _VP]),
     "nkr_b200_blind": (ctypes.c_int, [_VP, ctypes.POINTER(RawProofC), _VP, _VP,
                                       ctypes.POINTER(ProofC)]),
     "nkr_b200_key_intermediates": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
@@ -369,6 +379,60 @@ class MsmBases:
     def free(self):
         if self.h:
             _lib.nkr_b200_msm_bases_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def reduced_pairing(ctx, p_g1, q_g2):
+    """libff's reduced pairing of count (P, Q) pairs on the device: P G1 libff Jacobian
+    (count x 12 u64), Q G2 (count x 24 u64) -> GT (count x 48 u64, alt_bn128_Fq12)."""
+    p = np.ascontiguousarray(p_g1, dtype=np.uint64).reshape(-1, 12)
+    q = np.ascontiguousarray(q_g2, dtype=np.uint64).reshape(-1, 24)
+    if p.shape[0] != q.shape[0]:
+        raise ValueError("as many G1 as G2 points are needed")
+    out = np.zeros((p.shape[0], 48), np.uint64)
+    _check(_lib.nkr_b200_reduced_pairing(ctx.h, _ptr(p), _ptr(q), p.shape[0], _ptr(out)),
+           "nkr_b200_reduced_pairing")
+    return out
+
+
+class VerifyingKey:
+    """A verification key prepared on the device (nkr_b200_vk_prepare); verify_batch
+    is the reference's verify (protocol.cpp:96-108) for many proofs at once."""
+
+    def __init__(self, ctx, alpha_g1_beta_g2, gamma_g2, delta_g2, ic):
+        self.ctx = ctx
+        self._keep = [np.ascontiguousarray(x, dtype=np.uint64) for x in
+                      (alpha_g1_beta_g2, gamma_g2, delta_g2, ic)]
+        gt, g, d, icv = self._keep
+        self.n_ic = icv.size // 12
+        c = VerificationKeyC(gt.ctypes.data, g.ctypes.data, d.ctypes.data, icv.ctypes.data, self.n_ic)
+        h = _VP()
+        _check(_lib.nkr_b200_vk_prepare(ctx.h, ctypes.byref(c), ctypes.byref(h)), "nkr_b200_vk_prepare")
+        self.h = h
+
+    def verify_batch(self, public_inputs, proofs):
+        """public_inputs: count x n_public x 4 u64 (Fr Montgomery); proofs: count x 48 u64
+        (A, B, C libff Jacobian) -> bool array of verdicts."""
+        pr = np.ascontiguousarray(proofs, dtype=np.uint64).reshape(-1, 48)
+        count = pr.shape[0]
+        if count == 0:
+            return np.zeros(0, bool)
+        x = np.ascontiguousarray(public_inputs, dtype=np.uint64).reshape(count, -1)
+        n_public = x.shape[1] // 4
+        acc = np.zeros(count, np.uint8)
+        _check(_lib.nkr_b200_verify_batch(self.h, _ptr(x) if x.size else None, n_public, _ptr(pr),
+                                          count, _ptr(acc)), "nkr_b200_verify_batch")
+        return acc.astype(bool)
+
+    def free(self):
+        if self.h:
+            _lib.nkr_b200_vk_free(self.h)
             self.h = None
 
     def __del__(self):

@@ -281,6 +281,13 @@ class Ref:
         self._ok(f(_p(_arr(k)), _p(out)), "mul_gen")
         return out
 
+    def reduced_pairing(self, p_jac, q_jac):
+        """libff's reduced pairing (GT as 48 u64 Montgomery limbs) of libff Jacobian P, Q."""
+        out = np.zeros(48, np.uint64)
+        self._ok(self.lib.ref_reduced_pairing(_p(_arr(p_jac)), _p(_arr(q_jac)), _p(out)),
+                 "reduced_pairing")
+        return out
+
     def _circuit(self, r1cs):
         return Oracle._circuit(None, r1cs)
 
@@ -573,6 +580,20 @@ def write_proving_key(path, pk):
     for name in ("alpha_g1", "beta_g1", "beta_g2", "delta_g1", "delta_g2"):
         w.value(_arr(pk[name]).tobytes())
     w.close()
+
+
+def read_verification_key(path):
+    """A reference verification key artifact (common/src/io.cpp:72-77 over
+    BinaryArchive: magic, version, GT, gamma G2, delta G2, ic vector)."""
+    raw = open(path, "rb").read()
+    assert raw[:4] == b"LKZ1", "not a BinaryArchive file"
+    pos = 8
+    gt = np.frombuffer(raw[pos:pos + 384], np.uint64).copy(); pos += 384
+    gamma = np.frombuffer(raw[pos:pos + 192], np.uint64).copy(); pos += 192
+    delta = np.frombuffer(raw[pos:pos + 192], np.uint64).copy(); pos += 192
+    n = int(np.frombuffer(raw[pos:pos + 8], np.uint64)[0]); pos += 8
+    ic = np.frombuffer(raw[pos:pos + n], np.uint64).copy().reshape(-1, 12)
+    return {"alpha_g1_beta_g2": gt, "gamma_g2": gamma, "delta_g2": delta, "ic": ic}
 
 
 def write_proof(path, a_jac, b_jac, c_jac):

@@ -206,6 +206,21 @@ int ref_g2_mul_gen(const void *k, void *out_affine)
     })
 }
 
+// libff's reduced pairing e(P, Q) (Curve::reduced_pairing, as protocol.cpp:105-107
+// uses it): P, Q libff Jacobian (96 / 192 B), out the GT element (alt_bn128_Fq12,
+// 384 B, Montgomery limbs).
+int ref_reduced_pairing(const void *p_jac, const void *q_jac, void *out)
+{
+    REF_TRY({
+        G1 a;
+        G2 b;
+        std::memcpy((void *)&a, p_jac, 96);
+        std::memcpy((void *)&b, q_jac, 192);
+        const GT e = Curve::reduced_pairing(a, b);
+        std::memcpy(out, (const void *)&e, 384);
+    })
+}
+
 int ref_check_witness(const RawCircuit *rc, const void *witness, uint64_t n, int *ok)
 {
     REF_TRY({
