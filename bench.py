@@ -871,6 +871,97 @@ def run_kernels(args):
     ctx.close()
 
 
+# verification: circuits with few (sql-aggregate 1024: 4) and many (matmul 32: 3072)
+# public inputs
+VERIFY_WORKLOADS = [("sql-aggregate", 1024, 2), ("matmul", 32, 0)]
+
+
+def _uniform_fr_rows(rng, n):
+    """n uniform Fr elements (Montgomery limbs), rejection of values >= r"""
+    import numpy as np
+    r = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+    out = np.zeros((n, 4), np.uint64)
+    k = 0
+    while k < n:
+        v = int.from_bytes(rng.bytes(32), "little") & ((1 << 254) - 1)
+        if v < r:
+            out[k] = np.frombuffer(v.to_bytes(32, "little"), np.uint64)
+            k += 1
+    return out
+
+
+def run_verify(args):
+    """Groth16 verification throughput: nkr_b200_verify_batch over batches of valid
+    proofs (one raw proof blinded with many seeded r, s) against the reference's
+    own verify (common/src/protocol.cpp:96-108, oracle/_ref) on one host core."""
+    import numpy as np
+    import nkr_b200 as nk
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    ctx = nk.Context(0)
+    n = args.verify_batch
+    rng = np.random.default_rng(12)
+    rows_out = []
+    for kind, param, dens in VERIFY_WORKLOADS:
+        r1 = nk.generate(kind, param, dens, seed=1)
+        pk, vkp = nk.setup(ctx, r1, _seeded_toxic(77))
+        be = nk.Backend(ctx)
+        be.prepare(r1, pk)
+        del pk
+        raw = be.prove(r1.witness)
+        rs = _uniform_fr_rows(rng, 2 * n).reshape(n, 2, 4)
+        proofs = np.stack([np.frombuffer(bytes(be.blind(raw, r, s)), np.uint64) for r, s in rs])
+        pub = np.ascontiguousarray(r1.witness[1:1 + r1.public_inputs])
+        publics = np.ascontiguousarray(np.broadcast_to(pub, (n,) + pub.shape))
+        vk = nk.VerifyingKey(ctx, vkp["alpha_g1_beta_g2"], vkp["gamma_g2"], vkp["delta_g2"], vkp["ic"])
+        for _ in range(args.warmup):
+            ok = vk.verify_batch(publics, proofs)
+        assert ok.all(), "a valid proof was rejected"
+        clocks = ClockSampler(0)
+        clocks.start()
+        ts = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            vk.verify_batch(publics, proofs)
+            ts.append(time.perf_counter() - t)
+        clk = clocks.stop()
+        gpu_ps = n / statistics.median(ts)
+        # the reference verifier on one host core, a bounded sample of the same proofs
+        ref_ps = None
+        if not args.no_cpu_baseline:
+            import oracle as O
+            if O.ref_available():
+                ref = O.Ref()
+                with tempfile.TemporaryDirectory() as d:
+                    vk_path = os.path.join(d, "vk.bin")
+                    ref.write_vk(vkp, vk_path)
+                    done, t0 = 0, time.perf_counter()
+                    while done < 50 and time.perf_counter() - t0 < 10.0:
+                        pth = os.path.join(d, "p.bin")
+                        pr = proofs[done]
+                        O.write_proof(pth, pr[0:12], pr[12:36], pr[36:48])
+                        assert ref.verify(vk_path, pub, pth)
+                        done += 1
+                    ref_ps = done / (time.perf_counter() - t0)
+        rows_out.append({"workload": f"{kind} {param} ({r1.rows} constraints, "
+                                     f"{r1.public_inputs} public inputs)",
+                         "batch": n, "proofs_per_s": round(gpu_ps, 1),
+                         "ms_per_batch": round(statistics.median(ts) * 1e3, 3),
+                         "reference_cpu_1core_proofs_per_s": None if ref_ps is None else round(ref_ps, 2),
+                         "clocks": clk})
+        vk.free()
+        be.free()
+    line = {
+        "metric": "Groth16 verifications/s, batched (reference verdicts)", "value": rows_out[0]["proofs_per_s"],
+        "unit": "proofs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": "bn254 (exact modular; u32 limbs)",
+        "data": "synthetic (seeded circuits, witnesses, toxic waste, r and s)",
+        "config": {"workloads": rows_out,
+                   "path": "nkr_b200_verify_batch from host memory (proof and public-input "
+                           "upload, vk_x, Miller loop, final exponentiation, verdict download)"},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -879,12 +970,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="poseidon2048", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="prove", choices=["prove", "batch", "serve", "kernels"],
+    ap.add_argument("--mode", default="prove", choices=["prove", "batch", "serve", "kernels", "verify"],
                     help="prove: the 2^20 prove (default line); batch: 64 uneven proofs batched vs "
                          "plain; serve: Poisson requests over resident keys, server vs plain FIFO")
     ap.add_argument("--cases", default="all",
                     help="kernels mode: comma-separated subset, e.g. ntt.20,msm.g1.uniform.18 "
                          "(ntt.{16,20,24}; msm.g1.{uniform,sparse}.{16,18,20,22}; msm.g2.uniform.18)")
+    ap.add_argument("--verify-batch", type=int, default=8192)
     ap.add_argument("--serve-keys", type=int, default=6)
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.8)
@@ -898,6 +990,8 @@ def main():
         run_serve(args)
     elif args.mode == "kernels":
         run_kernels(args)
+    elif args.mode == "verify":
+        run_verify(args)
     else:
         run_b200(args)
 

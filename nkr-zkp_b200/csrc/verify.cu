@@ -10,7 +10,11 @@
 // e(alpha, beta): the same equation in GT, since the final exponentiation is a
 // homomorphism.  gamma and delta are fixed per key, so their Miller-loop lines
 // are computed once when the key is prepared; per proof only B's lines are
-// computed (affine, one Fq2 inversion per line).
+// computed (affine, one Fq2 inversion per line).  vk_x is a multi-scalar
+// multiplication over the key's fixed ic points: the key holds the 4-bit window
+// multiples d 2^(4w) ic[j + 1] (w < 64, d < 16, affine), and one warp per proof
+// sums the looked-up points of its public inputs (k_vk_x) before the pairing
+// kernel runs.
 #define NKR_FIELD_MUL_OUTLINE 1
 #include <cstring>
 
@@ -24,6 +28,7 @@ struct nkr_b200_vk {
     nkr::DevBuf ic;    // ic[] as G1 affine (R domain)
     nkr::DevBuf lines; // kAteLines lines of gamma, then of delta
     nkr::DevBuf flags; // int[2]: gamma, delta at infinity
+    nkr::DevBuf tab;   // [n_ic - 1][64][15] affine d 2^(4w) ic[j + 1]
     nkr::DevBuf io;    // batch staging (grown on demand)
 };
 
@@ -32,6 +37,7 @@ namespace nkr {
 namespace {
 
 constexpr size_t kProofBytes = 96 + 192 + 96; // A, B, C in libff layout
+constexpr int kIcWin = 64, kIcDig = 15;       // 4-bit windows of a public input
 
 // libff Jacobian (X, Y, Z) -> affine; Z = 0 is infinity
 template <class F>
@@ -56,6 +62,70 @@ __global__ void __launch_bounds__(32) k_vk_setup(const Fq2 *gd_jac, const Fq *ic
         flags[lane] = q.is_inf() ? 1 : 0;
         if (!q.is_inf()) ate_lines(q, lines + lane * kAteLines);
     }
+}
+
+// Q_{j,w} = 2^(4w) ic[j + 1]: thread j runs the doubling chain (XYZZ scratch)
+__global__ void __launch_bounds__(64) k_ic_pow(const G1Affine *ic, uint64_t n_pub, G1Xyzz *pow)
+{
+    const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n_pub) return;
+    const G1Affine p = ic[j + 1];
+    G1Xyzz q = p.is_inf() ? G1Xyzz::inf() : G1Xyzz{p.x, p.y, Fq::one(), Fq::one()};
+    for (int w = 0; w < kIcWin; ++w) {
+        pow[j * kIcWin + w] = q;
+        if (w + 1 < kIcWin)
+            for (int d = 0; d < 4; ++d) q = xyzz_dbl(q);
+    }
+}
+
+// tab[(j * 64 + w) * 15 + d - 1] = d Q_{j,w}, affine
+__global__ void __launch_bounds__(64) k_ic_entries(const G1Xyzz *pow, uint64_t count, G1Affine *tab)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const G1Xyzz q = pow[i / kIcDig];
+    const int d = int(i % kIcDig) + 1;
+    G1Xyzz acc = G1Xyzz::inf();
+    for (int b = 3; b >= 0; --b) {
+        acc = xyzz_dbl(acc);
+        if ((d >> b) & 1) acc = xyzz_add(acc, q);
+    }
+    tab[i] = xyzz_to_affine(acc);
+}
+
+// vk_x of proof i = ic[0] + sum_j x_ij ic[j + 1], one warp per proof: lane l sums
+// the table points of public inputs l, l + 32, ...; the warp adds its lanes'
+// sums; lane 0 writes the affine result.
+__device__ __forceinline__ G1Xyzz shfl_down_g1(const G1Xyzz &p, int off)
+{
+    G1Xyzz r;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        r.x.v[k] = __shfl_down_sync(0xffffffffu, p.x.v[k], off);
+        r.y.v[k] = __shfl_down_sync(0xffffffffu, p.y.v[k], off);
+        r.zz.v[k] = __shfl_down_sync(0xffffffffu, p.zz.v[k], off);
+        r.zzz.v[k] = __shfl_down_sync(0xffffffffu, p.zzz.v[k], off);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(128) k_vk_x(const G1Affine *ic, const G1Affine *tab, uint64_t n_pub,
+                                              const Fr *publics, uint64_t count, G1Affine *vk_x)
+{
+    const uint64_t i = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= count) return; // whole warps: count is per warp
+    G1Xyzz acc = G1Xyzz::inf();
+    for (uint64_t j = lane; j < n_pub; j += 32) {
+        const Fr x = from_mont(publics[i * n_pub + j]);
+        const G1Affine *t = tab + j * (kIcWin * kIcDig);
+        for (int w = 0; w < kIcWin; ++w) {
+            const int d = int((x.v[w >> 3] >> (4 * (w & 7))) & 15u);
+            if (d) acc = xyzz_add_affine(acc, t[w * kIcDig + d - 1]);
+        }
+    }
+    for (int off = 16; off; off >>= 1) acc = xyzz_add(acc, shfl_down_g1(acc, off));
+    if (lane == 0) vk_x[i] = xyzz_to_affine(xyzz_add_affine(acc, ic[0]));
 }
 
 // reduced pairings of count (P, Q) pairs, one per thread
@@ -83,11 +153,10 @@ __global__ void __launch_bounds__(64) k_pairing(const Fq *p_jac, const Fq2 *q_ja
 }
 
 // One proof per thread: proofs[i] = A (G1), B (G2), C (G1) in libff layout;
-// publics[i * n_pub + j] = x_j (Fr, Montgomery).
-__global__ void __launch_bounds__(64) k_verify(const Fq12 *gt, const G1Affine *ic, uint64_t n_ic,
+// vk_x[i] from k_vk_x.
+__global__ void __launch_bounds__(64) k_verify(const Fq12 *gt, const G1Affine *vk_x,
                                                const AteLine *lines, const int *flags,
-                                               const uint8_t *proofs, const Fr *publics,
-                                               uint64_t count, uint8_t *accept)
+                                               const uint8_t *proofs, uint64_t count, uint8_t *accept)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -95,14 +164,7 @@ __global__ void __launch_bounds__(64) k_verify(const Fq12 *gt, const G1Affine *i
     const Affine<Fq> a = libff_to_affine(reinterpret_cast<const Fq *>(pr));
     const Affine<Fq2> b = libff_to_affine(reinterpret_cast<const Fq2 *>(pr + 96));
     const Affine<Fq> c = libff_to_affine(reinterpret_cast<const Fq *>(pr + 288));
-    // vk_x = ic[0] + sum_j x_j ic[j + 1]
-    G1Xyzz acc = ic[0].is_inf() ? G1Xyzz::inf() : G1Xyzz{ic[0].x, ic[0].y, Fq::one(), Fq::one()};
-    const uint64_t n_pub = n_ic - 1;
-    for (uint64_t j = 0; j < n_pub; ++j) {
-        const Fr x = from_mont(publics[i * n_pub + j]);
-        acc = xyzz_add(acc, xyzz_mul_canon(ic[j + 1], x.v));
-    }
-    const Affine<Fq> nvk = g1_neg(xyzz_to_affine(acc));
+    const Affine<Fq> nvk = g1_neg(vk_x[i]);
     const Affine<Fq> nc = g1_neg(c);
     const bool on1 = !a.is_inf() && !b.is_inf();
     const bool on2 = !nvk.is_inf() && !flags[0];
@@ -165,6 +227,19 @@ int nkr_b200_vk_prepare(nkr_b200_ctx *ctx, const nkr_b200_verification_key *vk, 
                                  vk->n_ic, key->lines.as<AteLine>(), key->flags.as<int>(),
                                  key->ic.as<G1Affine>());
     NKR_CHECK_LAUNCH();
+    const uint64_t n_pub = vk->n_ic - 1;
+    if (n_pub) {
+        const uint64_t entries = n_pub * kIcWin * kIcDig;
+        NKR_TRY(key->tab.alloc(entries * sizeof(G1Affine), "ic window tables"));
+        DevBuf pow;
+        NKR_TRY(pow.alloc(n_pub * kIcWin * sizeof(G1Xyzz), "ic window powers"));
+        k_ic_pow<<<blocks_for(n_pub, 64), 64, 0, st>>>(key->ic.as<G1Affine>(), n_pub, pow.as<G1Xyzz>());
+        NKR_CHECK_LAUNCH();
+        k_ic_entries<<<blocks_for(entries, 64), 64, 0, st>>>(pow.as<G1Xyzz>(), entries,
+                                                             key->tab.as<G1Affine>());
+        NKR_CHECK_LAUNCH();
+        NKR_CUDA(cudaStreamSynchronize(st)); // pow is released on return
+    }
     NKR_CUDA(cudaStreamSynchronize(st));
     *out = key.release();
     return NKR_B200_OK;
@@ -183,17 +258,21 @@ int nkr_b200_verify_batch(nkr_b200_vk *vk, const void *public_inputs, uint64_t n
     }
     NKR_CUDA(cudaSetDevice(vk->ctx->device));
     cudaStream_t st = vk->ctx->stream;
-    const uint64_t pb = count * kProofBytes, xb = count * n_public * 32;
-    NKR_TRY(vk->io.alloc(pb + xb + count, "verification batch"));
+    // staging: proofs | public inputs | vk_x (affine) | verdicts
+    const uint64_t pb = count * kProofBytes, xb = count * n_public * 32, vb = count * sizeof(G1Affine);
+    NKR_TRY(vk->io.alloc(pb + xb + vb + count, "verification batch"));
     uint8_t *dp = vk->io.as<uint8_t>();
+    G1Affine *vkx = reinterpret_cast<G1Affine *>(dp + pb + xb);
+    uint8_t *acc = dp + pb + xb + vb;
     NKR_CUDA(cudaMemcpyAsync(dp, proofs, pb, cudaMemcpyHostToDevice, st));
     if (xb) NKR_CUDA(cudaMemcpyAsync(dp + pb, public_inputs, xb, cudaMemcpyHostToDevice, st));
-    k_verify<<<blocks_for(count, 64), 64, 0, st>>>(vk->gt.as<Fq12>(), vk->ic.as<G1Affine>(), vk->n_ic,
-                                                   vk->lines.as<AteLine>(), vk->flags.as<int>(), dp,
-                                                   reinterpret_cast<const Fr *>(dp + pb), count,
-                                                   dp + pb + xb);
+    k_vk_x<<<blocks_for(count * 32, 128), 128, 0, st>>>(vk->ic.as<G1Affine>(), vk->tab.as<G1Affine>(), n_public,
+                                                       reinterpret_cast<const Fr *>(dp + pb), count, vkx);
     NKR_CHECK_LAUNCH();
-    NKR_CUDA(cudaMemcpyAsync(accept, dp + pb + xb, count, cudaMemcpyDeviceToHost, st));
+    k_verify<<<blocks_for(count, 64), 64, 0, st>>>(vk->gt.as<Fq12>(), vkx, vk->lines.as<AteLine>(),
+                                                   vk->flags.as<int>(), dp, count, acc);
+    NKR_CHECK_LAUNCH();
+    NKR_CUDA(cudaMemcpyAsync(accept, acc, count, cudaMemcpyDeviceToHost, st));
     NKR_CUDA(cudaStreamSynchronize(st));
     return NKR_B200_OK;
 }

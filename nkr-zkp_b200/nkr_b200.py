@@ -551,7 +551,8 @@ def setup(ctx, r1cs, toxic):
     """GPU setup with toxic waste Fr[5] = (t, alpha, beta, gamma, delta).
 
     Returns (pk, vk_parts): pk in the proving-key dict layout Backend.prepare takes
-    (libff Jacobian arrays); vk_parts holds ic, gamma_g2, delta_g2, alpha_g1, beta_g2."""
+    (libff Jacobian arrays); vk_parts holds ic, gamma_g2, delta_g2, alpha_g1, beta_g2 and
+    alpha_g1_beta_g2 (e(alpha, beta), computed on the device)."""
     cols, rows = r1cs.cols, r1cs.rows
     arrs = {
         "a_query": np.zeros((cols, 12), np.uint64), "b_g1_query": np.zeros((cols, 12), np.uint64),
@@ -571,6 +572,8 @@ def setup(ctx, r1cs, toxic):
     pk = {k: arrs[k] for k in ("a_query", "b_g1_query", "b_g2_query", "l_query", "h_query",
                                "alpha_g1", "beta_g1", "delta_g1", "beta_g2", "delta_g2")}
     vk = {k: arrs[k] for k in ("ic", "gamma_g2", "delta_g2", "alpha_g1", "beta_g2")}
+    # the key's e(alpha, beta), as the reference's setup stores it (libff's GT value)
+    vk["alpha_g1_beta_g2"] = reduced_pairing(ctx, vk["alpha_g1"], vk["beta_g2"])[0]
     return pk, vk
 
 

@@ -125,3 +125,21 @@ def test_verify_public_input_count_mismatch_rejects(golden):
     got = vk.verify_batch(np.stack([np.concatenate([pub, pub[:1]])] * 2), np.stack([good, good]))
     assert not got.any()
     assert vk.verify_batch(np.zeros((0, 4 * len(pub)), np.uint64), np.zeros((0, 48), np.uint64)).size == 0
+
+
+def test_gpu_setup_key_verifies_its_proofs(ctx, ref):
+    """Setup, prove, blind and verify all on the device: the setup's e(alpha, beta)
+    equals libff's, and its key accepts the blinded proofs of its circuit."""
+    r1 = nk.generate("poseidon", 3, 2, seed=8)
+    pk, vkp = nk.setup(ctx, r1, O.random_fr(5, np.random.default_rng(46)))
+    assert np.array_equal(vkp["alpha_g1_beta_g2"], ref.reduced_pairing(vkp["alpha_g1"], vkp["beta_g2"]))
+    be = nk.Backend(ctx)
+    be.prepare(r1, pk)
+    raw = be.prove(r1.witness)
+    rs = O.random_fr(8, np.random.default_rng(47)).reshape(4, 2, 4)
+    proofs = np.stack([_proof_array(be.blind(raw, r, s)) for r, s in rs])
+    vk = nk.VerifyingKey(ctx, vkp["alpha_g1_beta_g2"], vkp["gamma_g2"], vkp["delta_g2"], vkp["ic"])
+    pub = np.ascontiguousarray(r1.witness[1:1 + r1.public_inputs])
+    assert vk.verify_batch(np.stack([pub] * 4), proofs).all()
+    vk.free()
+    be.free()
