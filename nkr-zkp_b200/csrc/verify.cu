@@ -10,7 +10,7 @@
 // e(alpha, beta): the same equation in GT, since the final exponentiation is a
 // homomorphism.  gamma and delta are fixed per key, so their Miller-loop lines
 // are computed once when the key is prepared; per proof only B's lines are
-// computed (affine, one Fq2 inversion per line).  vk_x is a multi-scalar
+// computed (homogeneous coordinates, no inversion).  vk_x is a multi-scalar
 // multiplication over the key's fixed ic points: the key holds the 4-bit window
 // multiples d 2^(4w) ic[j + 1] (w < 64, d < 16, affine), and one warp per proof
 // sums the looked-up points of its public inputs (k_vk_x) before the pairing
@@ -141,14 +141,14 @@ __global__ void __launch_bounds__(64) k_pairing(const Fq *p_jac, const Fq2 *q_ja
         return;
     }
     Fq12 f = fq12_one();
-    Affine<Fq2> t = q;
+    G2Proj t{q.x, q.y, Fq2::one()};
     for (int b = kAteTopBit - 1; b >= 0; --b) {
         f = sqr(f);
-        f = apply_line(f, ate_double(t), p);
-        if (ate_bit(b)) f = apply_line(f, ate_add(t, q), p);
+        f = apply_proj_line(f, proj_double(t, p));
+        if (ate_bit(b)) f = apply_proj_line(f, proj_add(t, q, p));
     }
-    f = apply_line(f, ate_add(t, twist_frobenius(q)), p);
-    f = apply_line(f, ate_add(t, twist_neg_frobenius2(q)), p);
+    f = apply_proj_line(f, proj_add(t, twist_frobenius(q), p));
+    f = apply_proj_line(f, proj_add(t, twist_neg_frobenius2(q), p));
     out[i] = final_exponentiation(f);
 }
 
@@ -171,23 +171,23 @@ __global__ void __launch_bounds__(64) k_verify(const Fq12 *gt, const G1Affine *v
     const bool on3 = !nc.is_inf() && !flags[1];
     const AteLine *lg = lines, *ld = lines + kAteLines;
     Fq12 f = fq12_one();
-    Affine<Fq2> t = b;
+    G2Proj t{b.x, b.y, Fq2::one()};
     int s = 0;
     for (int bit = kAteTopBit - 1; bit >= 0; --bit) {
         f = sqr(f);
-        if (on1) f = apply_line(f, ate_double(t), a);
+        if (on1) f = apply_proj_line(f, proj_double(t, a));
         if (on2) f = apply_line(f, lg[s], nvk);
         if (on3) f = apply_line(f, ld[s], nc);
         ++s;
         if (ate_bit(bit)) {
-            if (on1) f = apply_line(f, ate_add(t, b), a);
+            if (on1) f = apply_proj_line(f, proj_add(t, b, a));
             if (on2) f = apply_line(f, lg[s], nvk);
             if (on3) f = apply_line(f, ld[s], nc);
             ++s;
         }
     }
     for (int k = 0; k < 2; ++k, ++s) {
-        if (on1) f = apply_line(f, ate_add(t, k == 0 ? twist_frobenius(b) : twist_neg_frobenius2(b)), a);
+        if (on1) f = apply_proj_line(f, proj_add(t, k == 0 ? twist_frobenius(b) : twist_neg_frobenius2(b), a));
         if (on2) f = apply_line(f, lg[s], nvk);
         if (on3) f = apply_line(f, ld[s], nc);
     }

@@ -109,3 +109,46 @@ def reduced_pairing_limbs(p_jac, q_jac):
     P = (fq_int(p_jac[0:4]), fq_int(p_jac[4:8]))
     Q = ((fq_int(q_jac[0:4]), fq_int(q_jac[4:8])), (fq_int(q_jac[8:12]), fq_int(q_jac[12:16])))
     return gt_limbs(final_exp(miller(P, Q)))
+
+
+# libff's last chunk (alt_bn128_pairing.cpp:152-224) as the device computes it:
+# Frobenius maps x^(q^k) with xi^(m (q^k - 1)/6) on the coefficient of w^m, and the
+# addition chain with three exponentiations by -z.
+def _f2pow(a, e):
+    res = (1, 0)
+    while e:
+        if e & 1:
+            res = f2mul(res, a)
+        a = f2mul(a, a)
+        e >>= 1
+    return res
+
+
+GAMMA = {k: [_f2pow(XI, m * (q**k - 1) // 6) for m in range(6)] for k in (1, 2, 3)}
+
+
+def frobenius(xv, k):
+    def co(a, m):
+        b = f2conj(a) if k % 2 else a
+        return f2mul(b, GAMMA[k][m])
+    c0, c1 = xv
+    return (tuple(co(c0[i], 2 * i) for i in range(3)), tuple(co(c1[i], 2 * i + 1) for i in range(3)))
+
+
+def exp_by_neg_z(xv):
+    return f12conj(f12pow(xv, x))
+
+
+def final_exp_chain(f):
+    c = f12mul(f12conj(f), f12inv(f))
+    elt = f12mul(frobenius(c, 2), c)
+    A = exp_by_neg_z(elt)
+    B = f12mul(A, A)
+    D = f12mul(f12mul(B, B), B)
+    E = exp_by_neg_z(D)
+    G = exp_by_neg_z(f12mul(E, E))
+    K = f12mul(f12mul(f12conj(G), E), f12conj(D))
+    L = f12mul(K, B)
+    N = f12mul(f12mul(K, E), elt)
+    R = f12mul(frobenius(K, 2), f12mul(frobenius(L, 1), N))
+    return f12mul(frobenius(f12mul(f12conj(elt), L), 3), R)
