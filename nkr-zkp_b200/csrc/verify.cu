@@ -269,7 +269,9 @@ int nkr_b200_verify_batch(nkr_b200_vk *vk, const void *public_inputs, uint64_t n
     k_vk_x<<<blocks_for(count * 32, 128), 128, 0, st>>>(vk->ic.as<G1Affine>(), vk->tab.as<G1Affine>(), n_public,
                                                        reinterpret_cast<const Fr *>(dp + pb), count, vkx);
     NKR_CHECK_LAUNCH();
-    k_verify<<<blocks_for(count, 64), 64, 0, st>>>(vk->gt.as<Fq12>(), vkx, vk->lines.as<AteLine>(),
+    // one warp per block: at 255 registers an SM holds 8 such blocks, and a batch
+    // spreads over every SM before any SM takes a second warp
+    k_verify<<<blocks_for(count, 32), 32, 0, st>>>(vk->gt.as<Fq12>(), vkx, vk->lines.as<AteLine>(),
                                                    vk->flags.as<int>(), dp, count, acc);
     NKR_CHECK_LAUNCH();
     NKR_CUDA(cudaMemcpyAsync(accept, acc, count, cudaMemcpyDeviceToHost, st));
