@@ -1,6 +1,5 @@
-// Groth16 prepare / prove / blind on one B200 (design notes in prover.cuh).
-// Curve arithmetic in the finishing kernels: out-of-line products.
-#define NKR_FIELD_MUL_OUTLINE 1
+// Groth16 prepare / prove orchestration on one B200 (design notes in
+// prover.cuh); the blinding kernels live in blind.cu, verification in verify.cu.
 #include <algorithm>
 #include <cstring>
 #include <vector>
