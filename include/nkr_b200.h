@@ -277,6 +277,13 @@ int nkr_b200_msm_g2(nkr_b200_ctx *ctx, const void *bases, const void *scalars, u
 int nkr_b200_tune_ntt(nkr_b200_ctx *ctx, uint64_t n, int *max_stages, int *bfly_per_thread);
 int nkr_b200_set_autotune(nkr_b200_ctx *ctx, int enable);
 int nkr_b200_tune_msm(nkr_b200_ctx *ctx, uint64_t n, int *window_bits, float *ms);
+/* Measured MSM window widths persist across processes (the reference's CLI proves
+ * once per process and would otherwise re-measure on every run):
+ * nkr_b200_tune_save writes this context's measured size classes to a text file;
+ * nkr_b200_tune_load takes them back (loaded = size classes read), refusing a file
+ * written on a different device model or SM count. */
+int nkr_b200_tune_save(nkr_b200_ctx *ctx, const char *path);
+int nkr_b200_tune_load(nkr_b200_ctx *ctx, const char *path, int *loaded);
 
 /* Resident-bases MSM (the prove path's form): bases uploaded and expanded once
  * into per-window copies, then any number of MSMs with new scalars. */

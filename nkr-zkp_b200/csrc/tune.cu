@@ -7,6 +7,7 @@
 // the model's c and its neighbours, once per power-of-two size class, and keeps
 // the fastest.  Any c gives the same (canonical) result.
 #define NKR_FIELD_MUL_OUTLINE 1
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -157,3 +158,89 @@ int tuned_window_bits(nkr_b200_ctx *ctx, uint64_t n, int *c)
 }
 
 } // namespace nkr
+
+// Tuned widths persist across processes: the reference's CLI proves once per
+// process (app/prove.cpp:70-88), and every process would otherwise measure the
+// same size classes again (about 1.6 s for a 2^20 key's classes).  Text file:
+//   nkr-b200-tune 1
+//   device <cudaDeviceProp::name>
+//   sms <multiprocessor count>
+//   msm <log2 size class> <window bits> <ms>     (one line per measured class)
+namespace nkr {
+
+namespace {
+
+int device_identity(const nkr_b200_ctx *ctx, char *name, size_t len)
+{
+    cudaDeviceProp prop{};
+    NKR_CUDA(cudaGetDeviceProperties(&prop, ctx->device));
+    std::snprintf(name, len, "%s", prop.name);
+    return NKR_B200_OK;
+}
+
+} // namespace
+
+} // namespace nkr
+
+extern "C" {
+
+int nkr_b200_tune_save(nkr_b200_ctx *ctx, const char *path)
+{
+    NKR_REQUIRE(ctx && path, "null argument");
+    char name[256];
+    NKR_TRY(nkr::device_identity(ctx, name, sizeof name));
+    FILE *f = std::fopen(path, "w");
+    NKR_REQUIRE(f, "%s: cannot open for writing", path);
+    bool ok = std::fprintf(f, "nkr-b200-tune 1\ndevice %s\nsms %d\n", name, ctx->sm_count) > 0;
+    for (int lg = 0; lg < 33 && ok; ++lg)
+        if (ctx->msm_window[lg])
+            ok = std::fprintf(f, "msm %d %d %.6f\n", lg, ctx->msm_window[lg], ctx->msm_window_ms[lg]) > 0;
+    ok = (std::fclose(f) == 0) && ok;
+    NKR_REQUIRE(ok, "%s: write failed", path);
+    return NKR_B200_OK;
+}
+
+int nkr_b200_tune_load(nkr_b200_ctx *ctx, const char *path, int *loaded)
+{
+    NKR_REQUIRE(ctx && path, "null argument");
+    if (loaded) *loaded = 0;
+    char name[256];
+    NKR_TRY(nkr::device_identity(ctx, name, sizeof name));
+    FILE *f = std::fopen(path, "r");
+    NKR_REQUIRE(f, "%s: cannot open", path);
+    char line[512];
+    int version = 0, sms = -1, n = 0, window[33] = {};
+    float ms[33] = {};
+    bool same_device = false, bad = false;
+    while (std::fgets(line, sizeof line, f)) {
+        line[std::strcspn(line, "\r\n")] = 0;
+        int lg = 0, c = 0;
+        float t = 0.f;
+        if (std::sscanf(line, "nkr-b200-tune %d", &version) == 1) continue;
+        if (std::strncmp(line, "device ", 7) == 0) {
+            same_device = std::strcmp(line + 7, name) == 0;
+        } else if (std::sscanf(line, "sms %d", &sms) == 1) {
+        } else if (std::sscanf(line, "msm %d %d %f", &lg, &c, &t) == 3) {
+            if (lg < 0 || lg > 32 || c < 6 || c > 22) bad = true;
+            else {
+                window[lg] = c;
+                ms[lg] = t;
+                ++n;
+            }
+        } else if (line[0]) {
+            bad = true;
+        }
+    }
+    std::fclose(f);
+    NKR_REQUIRE(version == 1 && !bad, "%s: not a tuning file of this library", path);
+    NKR_REQUIRE(same_device && sms == ctx->sm_count, "%s: measured on another device", path);
+    for (int lg = 0; lg < 33; ++lg)
+        if (window[lg]) {
+            ctx->msm_window[lg] = window[lg];
+            ctx->msm_window_ms[lg] = ms[lg];
+        }
+    if (loaded) *loaded = n;
+    return NKR_B200_OK;
+}
+
+} // extern "C"

@@ -9,6 +9,7 @@
 // points the ABI structs at the reference's std::vector data: CsrMatrix
 // (r1cs/spmat.hpp:206-215), libff Fr / G1 / G2 (types.hpp:11-15), RawProof
 // (types.hpp:47-53).
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -64,7 +65,17 @@ nkr_b200_proving_key key_view(const ProvingKey &pk)
 
 class B200Backend final : public Backend {
 public:
-    B200Backend() { check(nkr_b200_open(0, &ctx_), "open"); }
+    // NKR_B200_TUNE_CACHE names a file of measured MSM window widths, kept across
+    // the CLI's one-proof processes (a missing or foreign file is measured afresh)
+    B200Backend()
+    {
+        check(nkr_b200_open(0, &ctx_), "open");
+        if (const char *p = std::getenv("NKR_B200_TUNE_CACHE")) {
+            tune_cache_ = p;
+            int n = 0;
+            (void)nkr_b200_tune_load(ctx_, p, &n);
+        }
+    }
     ~B200Backend() override
     {
         nkr_b200_key_free(key_);
@@ -117,6 +128,7 @@ public:
         const nkr_b200_proving_key kv = key_view(pk);
         check(nkr_b200_prepare(ctx_, &cv, &kv, &key_), "prepare");
         prepared_for_ = &circuit;
+        if (!tune_cache_.empty()) (void)nkr_b200_tune_save(ctx_, tune_cache_.c_str());
     }
 
     // Backend::prove: raw proof points, affine-normalised libff Jacobian layout.
@@ -137,6 +149,7 @@ private:
     nkr_b200_ctx *ctx_ = nullptr;
     nkr_b200_key *key_ = nullptr;
     const Circuit *prepared_for_ = nullptr;
+    std::string tune_cache_;
 };
 
 } // namespace

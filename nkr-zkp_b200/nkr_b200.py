@@ -90,6 +90,8 @@ _SIGS = {
     "nkr_b200_key_free": (None, [_VP]),
     "nkr_b200_key_device_bytes": (_U64, [_VP]),
     "nkr_b200_prove": (ctypes.c_int, [_VP, _VP, _U64, ctypes.POINTER(RawProofC)]),
+    "nkr_b200_tune_save": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "nkr_b200_tune_load": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
     "nkr_b200_vk_prepare": (ctypes.c_int, [_VP, ctypes.POINTER(VerificationKeyC),
                                            ctypes.POINTER(_VP)]),
     "nkr_b200_verify_batch": (ctypes.c_int, [_VP, _VP, _U64, _VP, _U64, _VP]),
@@ -279,6 +281,16 @@ class Context:
             pass
 
     # operator-level entry points -------------------------------------------
+    def tune_save(self, path):
+        """Write the measured MSM window widths of this context (nkr_b200_tune_save)."""
+        _check(_lib.nkr_b200_tune_save(self.h, str(path).encode()), "nkr_b200_tune_save")
+
+    def tune_load(self, path):
+        """Load widths measured earlier on this device model; returns the size classes read."""
+        n = ctypes.c_int()
+        _check(_lib.nkr_b200_tune_load(self.h, str(path).encode(), ctypes.byref(n)), "nkr_b200_tune_load")
+        return n.value
+
     def ntt(self, op, data):
         d = _fr(data).copy()
         _check(_lib.nkr_b200_ntt(self.h, op, _ptr(d), d.size // 4), f"ntt op {op}")
