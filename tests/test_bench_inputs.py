@@ -32,3 +32,15 @@ def test_sparse_witness_mix_shape():
     assert 0.47 < zero < 0.53          # 30% + a third of 60%
     assert 0.18 < one < 0.22           # a third of 60%
     assert 0.09 < big < 0.11           # the uniform 10%
+
+
+def test_verify_mode_scalars_are_uniform_fr():
+    """bench.py's verify mode draws r, s as Fr Montgomery limbs below r, deterministically."""
+    import numpy as np
+    import bench
+    a = bench._uniform_fr_rows(np.random.default_rng(12), 64)
+    b = bench._uniform_fr_rows(np.random.default_rng(12), 64)
+    assert np.array_equal(a, b) and a.shape == (64, 4)
+    r = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+    vals = [sum(int(w) << (64 * i) for i, w in enumerate(row)) for row in a]
+    assert all(v < r for v in vals) and len(set(vals)) == 64
