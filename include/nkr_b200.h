@@ -156,8 +156,8 @@ int nkr_b200_blind(nkr_b200_key *key, const nkr_b200_raw_proof *raw, const void 
 /* ---- verification -------------------------------------------------------- */
 
 /* Prepares a verification key on the device (ic normalised, the Miller-loop
- * lines of gamma and delta computed once, and 4-bit window tables of the ic
- * points: 61 KB of device memory per public input).  A prepared key serves one
+ * lines of gamma and delta computed once, and signed 5-bit window tables of the
+ * ic points: 52 KB of device memory per public input).  A prepared key serves one
  * nkr_b200_verify_batch call at a time (its batch staging is per key). */
 int nkr_b200_vk_prepare(nkr_b200_ctx *ctx, const nkr_b200_verification_key *vk,
                         nkr_b200_vk **out);

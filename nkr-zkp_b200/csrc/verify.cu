@@ -11,8 +11,8 @@
 // homomorphism.  gamma and delta are fixed per key, so their Miller-loop lines
 // are computed once when the key is prepared; per proof only B's lines are
 // computed (homogeneous coordinates, no inversion).  vk_x is a multi-scalar
-// multiplication over the key's fixed ic points: the key holds the 4-bit window
-// multiples d 2^(4w) ic[j + 1] (w < 64, d < 16, affine), and one warp per proof
+// multiplication over the key's fixed ic points: the key holds the signed 5-bit
+// window multiples d 2^(5w) ic[j + 1] (w < 51, d = 1..16, affine), and one warp per proof
 // sums the looked-up points of its public inputs (k_vk_x, in the FP64 field)
 // before the pairing kernel runs.
 #define NKR_FIELD_MUL_OUTLINE 1
@@ -29,7 +29,7 @@ struct nkr_b200_vk {
     nkr::DevBuf ic;    // ic[] as G1 affine (R domain)
     nkr::DevBuf lines; // kAteLines lines of gamma, then of delta
     nkr::DevBuf flags; // int[2]: gamma, delta at infinity
-    nkr::DevBuf tab;   // [n_ic - 1][64][15] affine d 2^(4w) ic[j + 1], R' = 2^260 domain
+    nkr::DevBuf tab;   // [n_ic - 1][51][16] affine d 2^(5w) ic[j + 1], R' = 2^260 domain
     nkr::DevBuf io;    // batch staging (grown on demand)
 };
 
@@ -38,7 +38,7 @@ namespace nkr {
 namespace {
 
 constexpr size_t kProofBytes = 96 + 192 + 96; // A, B, C in libff layout
-constexpr int kIcWin = 64, kIcDig = 15;       // 4-bit windows of a public input
+constexpr int kIcWin = 51, kIcDig = 16;       // signed 5-bit windows of a public input
 
 // libff Jacobian (X, Y, Z) -> affine; Z = 0 is infinity
 template <class F>
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(32) k_vk_setup(const Fq2 *gd_jac, const Fq *ic
     }
 }
 
-// Q_{j,w} = 2^(4w) ic[j + 1]: thread j runs the doubling chain (XYZZ scratch)
+// Q_{j,w} = 2^(5w) ic[j + 1]: thread j runs the doubling chain (XYZZ scratch)
 __global__ void __launch_bounds__(64) k_ic_pow(const G1Affine *ic, uint64_t n_pub, G1Xyzz *pow)
 {
     const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(64) k_ic_pow(const G1Affine *ic, uint64_t n_pu
     for (int w = 0; w < kIcWin; ++w) {
         pow[j * kIcWin + w] = q;
         if (w + 1 < kIcWin)
-            for (int d = 0; d < 4; ++d) q = xyzz_dbl(q);
+            for (int d = 0; d < 5; ++d) q = xyzz_dbl(q);
     }
 }
 
@@ -86,7 +86,7 @@ __device__ __forceinline__ G1Affine affine_to_r260_storage(const G1Affine &a)
     return {from52(r256_to_r260(to52(a.x))), from52(r256_to_r260(to52(a.y)))};
 }
 
-// tab[(j * 64 + w) * 15 + d - 1] = d Q_{j,w}, affine in the R' domain
+// tab[(j * 51 + w) * 16 + d - 1] = d Q_{j,w} (d = 1..16), affine in the R' domain
 __global__ void __launch_bounds__(64) k_ic_entries(const G1Xyzz *pow, uint64_t count, G1Affine *tab)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(64) k_ic_entries(const G1Xyzz *pow, uint64_t c
     const G1Xyzz q = pow[i / kIcDig];
     const int d = int(i % kIcDig) + 1;
     G1Xyzz acc = G1Xyzz::inf();
-    for (int b = 3; b >= 0; --b) {
+    for (int b = 4; b >= 0; --b) {
         acc = xyzz_dbl(acc);
         if ((d >> b) & 1) acc = xyzz_add(acc, q);
     }
@@ -129,11 +129,19 @@ __global__ void __launch_bounds__(128, 3) k_vk_x(const G1Affine *ic, const G1Aff
     for (uint64_t j = lane; j < n_pub; j += 32) {
         const Fr x = from_mont(publics[i * n_pub + j]);
         const G1Affine *t = tab + j * (kIcWin * kIcDig);
+        // signed digits: v = bits + carry, v > 16 -> v - 32 (x < 2^254 leaves no carry)
+        uint32_t carry = 0;
         for (int w = 0; w < kIcWin; ++w) {
-            const int d = int((x.v[w >> 3] >> (4 * (w & 7))) & 15u);
+            const int off = 5 * w, limb = off >> 5, sh = off & 31;
+            uint64_t word = x.v[limb];
+            if (limb + 1 < 8) word |= uint64_t(x.v[limb + 1]) << 32;
+            const uint32_t v = (uint32_t(word >> sh) & 31u) + carry;
+            carry = v > 16 ? 1u : 0u;
+            const int d = v > 16 ? int(v) - 32 : int(v);
             if (d) {
-                const G1Affine e = t[w * kIcDig + d - 1];
-                acc = xyzz_add_affine(acc, Affine<Fq52>{to52(e.x), to52(e.y)});
+                const G1Affine e = t[w * kIcDig + (d < 0 ? -d : d) - 1];
+                const Affine<Fq52> p{to52(e.x), to52(e.y)};
+                acc = xyzz_add_affine(acc, d < 0 ? affine_neg(p) : p);
             }
         }
     }
