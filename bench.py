@@ -17,12 +17,17 @@ of a fresh seeded witness on resident keys.
   roofline  the dominant kernel (MSM bucket accumulation) in Fq-multiplications/s
             against this GPU's measured Montgomery-product throughput; HBM bytes
             of the same kernel against the measured copy bandwidth beside it.
-  cpu_baseline  the reference's own CPU prover (oracle/_ref, libff/libfqfft, one
-            thread as the reference runs it) on a bounded sample (poseidon 128,
-            2^16 constraints), scaled linearly to 2^20 constraints.
+  cpu_baseline  one single-threaded prove of the same circuit, key and witness by
+            the reference's own CPU prover (oracle/_ref: libff/libfqfft built from
+            the reference sources, one thread as the reference's bench runs it),
+            in its own process; its raw proof is compared with the GPU's.
 
---impl reference runs the reference CPU prover alone on the host cores (one
-process per core, each proving the 2^16 sample; ms per 2^20-equivalent proof).
+--impl reference runs the reference CPU prover alone on the host cores: the
+circuit built by the reference's own Poseidon gadget from the same seeded
+preimages, its own CPU setup, then m = min(cores, steps) single-threaded
+processes proving and blinding together (groth16.prove.total); value = T_max / m
+ms per proof (the reference bench's m / T_max throughput).  That arm loads
+nothing of this repository's library.
 Inputs (all > 126 MB L2 per prove: keys ~7 GB, witness 32 MB) are synthetic and
 seeded: circuit, witness and toxic waste come from seeded generators.
 """
@@ -46,7 +51,6 @@ WORKLOADS = {
     "matmul32": ("matmul", 32, 0),
 }
 METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
-REF_SAMPLE = ("poseidon", 128, 2)  # 2^16 constraints
 # DRAM read + write bytes per (point, digit) entry of the G1 accumulation kernel,
 # from an ncu capture at 2^18 points (a 2^20 capture would hold ~6 GB of keys on
 # the device); traffic grows with entries (one random base gather per entry)
@@ -153,112 +157,181 @@ def _seeded_toxic(seed):
     return out
 
 
-def cpu_baseline_reference(sample=REF_SAMPLE):
-    """Reference CPU prover on the bounded sample; returns (ms at 2^20 scale, description)."""
-    import numpy as np  # noqa: F401
+def _save_circuit(d, c):
+    """The circuit's CSR arrays and witness as .npy files a spawned process reloads."""
+    import numpy as np
+    np.save(os.path.join(d, "shape.npy"), np.array([c.rows, c.cols, c.public_inputs], np.uint64))
+    np.save(os.path.join(d, "witness.npy"), c.witness)
+    for k in range(3):
+        np.save(os.path.join(d, f"row_ptr{k}.npy"), c.row_ptr[k])
+        np.save(os.path.join(d, f"col_idx{k}.npy"), c.col_idx[k])
+        np.save(os.path.join(d, f"values{k}.npy"), c.values[k])
+
+
+def _load_circuit(d):
+    from types import SimpleNamespace
+    import numpy as np
+    rows, cols, pub = (int(v) for v in np.load(os.path.join(d, "shape.npy")))
+    return SimpleNamespace(
+        rows=rows, cols=cols, public_inputs=pub, witness=np.load(os.path.join(d, "witness.npy")),
+        row_ptr=[np.load(os.path.join(d, f"row_ptr{k}.npy")) for k in range(3)],
+        col_idx=[np.load(os.path.join(d, f"col_idx{k}.npy")) for k in range(3)],
+        values=[np.load(os.path.join(d, f"values{k}.npy")) for k in range(3)])
+
+
+def _ref_prove_process(circ_dir, pk_path, blind, barrier, results, idx):
+    """One reference CPU prove in its own spawned, single-threaded process
+    (OMP_NUM_THREADS=1 as the reference's bench runs it, scripts/bench/runner.py:
+    458-467).  Only oracle/_ref (the reference's CPU path built from its sources)
+    is loaded.  Circuit, witness and proving key load before the barrier, untimed;
+    the timer covers CpuBackend::prove (backends/cpu/src/backend.cpp:156-201) and,
+    with blind, the reference's blind_proof after it (groth16.prove.total of
+    app/prove.cpp:70-88).  Puts (idx, seconds, raw proof bytes or None)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import nkr_b200 as nk
     import oracle as O
-    kind, param, dens = sample
-    r1 = nk.generate(kind, param, dens, seed=1)
-    d = tempfile.mkdtemp()
-    if O.ref_available():
+    try:
+        c = _load_circuit(circ_dir)
         ref = O.Ref()
-        ref.cpu_setup(r1, os.path.join(d, "pk"), os.path.join(d, "vk"))
-        h = ref.prover(r1, os.path.join(d, "pk"))
-        reps = 2  # about 12 s of single-threaded CPU work
+        h = ref.prover(c, pk_path)
+        if barrier is not None:
+            barrier.wait(timeout=900)
         t0 = time.perf_counter()
-        for _ in range(reps):
-            ref.prover_prove(h, r1.witness)
-        dt = (time.perf_counter() - t0) / reps
-        ref.prover_close(h)
-        kind_s = "reference"
-    else:
-        orc = O.Oracle()
-        pk = {}
-        # oracle port: random bases suffice for timing
-        gen1, gen2 = orc.g1_generator(), orc.g2_generator()
-        import numpy as np
-        rng = np.random.default_rng(3)
-        k = O.random_fr(1, rng)[0]
-        p1, p2 = orc.mul_affine(1, gen1, k), orc.mul_affine(2, gen2, k)
-        for name, n, g in (("a_query", r1.cols, p1), ("b_g1_query", r1.cols, p1),
-                           ("b_g2_query", r1.cols, p2), ("l_query", r1.cols, p1),
-                           ("h_query", r1.rows, p1)):
-            pk[name] = np.tile(g, (n, 1))
-        for name, g in (("alpha_g1", p1), ("beta_g1", p1), ("delta_g1", p1), ("beta_g2", p2),
-                        ("delta_g2", p2)):
-            pk[name] = g
-        t0 = time.perf_counter()
-        orc.prove(r1, pk, r1.witness, threads=1)
+        if blind:
+            ref.prover_prove_blind(h, c.witness)
+            raw = None
+        else:
+            g1, g2 = ref.prover_prove(h, c.witness)
+            raw = g1.tobytes() + g2.tobytes()
         dt = time.perf_counter() - t0
-        kind_s = "port"
-    scale = (1 << 20) / r1.rows
-    return dt * 1e3 * scale, kind_s, (f"{kind} count={param} density=sparse ({r1.rows} constraints), "
-                                      f"single-threaded prove {dt:.2f} s (mean of the proves run), "
-                                      f"scaled x{scale:.0f} (linear in constraints) to 2^20")
+        ref.prover_close(h)
+        results.put((idx, dt, raw))
+    except Exception as e:  # reported by the parent
+        results.put((idx, None, repr(e)))
 
 
-def _ref_worker(args):
-    kind, param, dens, pk_path = args
-    sys.path.insert(0, os.path.join(ROOT, "nkr-zkp_b200"))
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import nkr_b200 as nk
-    import oracle as O
-    r1 = nk.generate(kind, param, dens, seed=1)
-    ref = O.Ref()
-    h = ref.prover(r1, pk_path)
-    t0 = time.perf_counter()
-    ref.prover_prove(h, r1.witness)
-    return time.perf_counter() - t0
+def _spawn_ref_proves(circ_dir, pk_path, m, blind):
+    """m concurrent single-threaded reference proves started together; returns
+    the per-process prove seconds (and the raw proofs without blinding)."""
+    import multiprocessing as mp
+    os.environ["OMP_NUM_THREADS"] = "1"
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(m) if m > 1 else None
+    results = ctx.Queue()
+    procs = [ctx.Process(target=_ref_prove_process,
+                         args=(circ_dir, pk_path, blind, barrier, results, i)) for i in range(m)]
+    for p in procs:
+        p.start()
+    out = [results.get(timeout=1800) for _ in range(m)]
+    for p in procs:
+        p.join(timeout=60)
+    bad = [o for o in out if o[1] is None]
+    if bad:
+        raise RuntimeError(f"reference prove failed: {bad[0][2]}")
+    return sorted(out)
+
+
+def _ref_workload(ref, workload):
+    """The bench workload built by the reference's own Poseidon gadget and
+    R1CSManager from the seeded preimages (identical to the repository's
+    generator output; tests/test_generator.py pins that)."""
+    kind, param, dens = WORKLOADS[workload]
+    if kind != "poseidon":
+        return None
+    return ref.poseidon_circuit_seeded(param, dens, 1)
+
+
+def _config(kind, param, dens, rows, cols, world):
+    return {"workload": f"groth16-prove {kind} count={param} density="
+                        f"{['full', 'hybrid', 'sparse'][dens]} ({rows} constraints, "
+                        f"{cols} variables padded)",
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (keys, witness); no flush"}
+
+
+DTYPE = "bn254 Fr/Fq (exact modular arithmetic)"
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU prover with every host core busy."""
+    """--impl reference: the reference's own CPU prover (oracle/_ref) on the same
+    2^20 workload, every host core busy, measured as the reference's bench
+    measures concurrent proves (scripts/bench/metrics.py:73-77: m proves started
+    together, throughput m / T_max), reported as ms per proof = T_max / m.  This
+    process and its workers load nothing of this repository's library."""
     world, rank, _ = _dist()
     if rank != 0:
         return
-    import multiprocessing as mp
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import nkr_b200 as nk
     import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the "
                           "reference source tree at build time)"}))
         return
-    cores = os.cpu_count() or 1
-    kind, param, dens = REF_SAMPLE
-    r1 = nk.generate(kind, param, dens, seed=1)
+    t_setup = time.perf_counter()
+    ref = O.Ref()
+    c = _ref_workload(ref, args.workload)
+    if c is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"--impl reference builds poseidon "
+                          f"workloads only (asked: {args.workload})"}))
+        return
+    kind, param, dens = WORKLOADS[args.workload]
     d = tempfile.mkdtemp()
-    O.Ref().cpu_setup(r1, os.path.join(d, "pk"), os.path.join(d, "vk"))
-    ctx = mp.get_context("spawn")
-    scale = (1 << 20) / r1.rows
-    with ctx.Pool(cores) as pool:
-        job = [(kind, param, dens, os.path.join(d, "pk"))] * cores
-        for _ in range(args.warmup):
-            pool.map(_ref_worker, job)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            pool.map(_ref_worker, job)
-        wall = time.perf_counter() - t0
-    ms_per_proof = wall * 1e3 / (args.steps * cores) * scale
+    pk_path = os.path.join(d, "pk.bin")
+    # the reference CPU setup (backend.cpp:41-154; its own unseeded toxic waste)
+    ref.cpu_setup(c, pk_path, os.path.join(d, "vk.bin"))
+    _save_circuit(d, c)
+    cores = len(os.sched_getaffinity(0))
+    try:
+        import psutil
+        mem_cap = int(psutil.virtual_memory().available // (3 << 30))  # ~1.2 GB per process at 2^20
+    except ImportError:
+        mem_cap = cores
+    m = max(1, min(cores, args.steps, mem_cap))
+    setup_s = time.perf_counter() - t_setup
+    t0 = time.perf_counter()
+    out = _spawn_ref_proves(d, pk_path, m, blind=True)
+    wall = time.perf_counter() - t0
+    secs = [o[1] for o in out]
+    t_max_ms = max(secs) * 1e3
+    ms_per_proof = t_max_ms / m
+    sample = (f"{m} concurrent single-threaded reference proves (CpuBackend::prove + blind_proof, "
+              f"the CLI's groth16.prove.total) of the full workload, one process per core, "
+              f"started together; value = T_max / m (metrics.py:73-77)")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(ms_per_proof, 3), "unit": "ms",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)",
-        "data": "synthetic (seeded circuit, witness and toxic waste)",
-        "config": {"workload": "groth16-prove poseidon count=2048 density=sparse (2^20 constraints)",
-                   "sample": f"{kind} count={param} sparse ({r1.rows} constraints) per process, "
-                             f"{cores} processes, scaled x{scale:.0f} to 2^20"},
-        "cpu_baseline": {"value": round(ms_per_proof, 3), "unit": "ms", "cores": cores,
-                         "kind": "reference",
-                         "sample": f"{cores} concurrent single-threaded reference proves of the "
-                                   f"2^16 sample per step, scaled linearly to 2^20"},
+        "ms_per_step": round(ms_per_proof, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
+        "data": "synthetic (seeded circuit and witness; the reference setup's own toxic waste)",
+        "config": _config(kind, param, dens, c.rows, c.cols, world),
+        "proofs_timed": m, "t_max_ms": round(t_max_ms, 1),
+        "latency_ms_median": round(statistics.median(secs) * 1e3, 1),
+        "warmup_note": "no warm-up proves: each process loads its circuit and key untimed before "
+                       "the common start; a CPU prove has no device state to warm",
+        "setup_s": round(setup_s, 1), "wall_s": round(wall, 1),
+        "cpu_baseline": {"value": round(ms_per_proof, 3), "unit": "ms", "cores": m,
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": round(ms_per_proof, 3), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def cpu_baseline_single(r1, pk, raw_gpu):
+    """The GPU line's CPU baseline: one single-threaded reference CPU prove
+    (oracle/_ref) of the same circuit, key and witness, in a spawned process.
+    Returns (ms, raw proofs equal)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return None
+    d = tempfile.mkdtemp()
+    pk_path = os.path.join(d, "pk.bin")
+    O.write_proving_key(pk_path, pk)
+    _save_circuit(d, r1)
+    out = _spawn_ref_proves(d, pk_path, 1, blind=False)
+    _, secs, raw = out[0]
+    same = raw == raw_gpu
+    return secs * 1e3, same
 
 
 def run_b200(args):
@@ -292,7 +365,9 @@ def run_b200(args):
         prep_ms.append((time.perf_counter() - t0) * 1e3)
         if i < 2:
             be.free()
-    del pk
+    want_cpu = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if not want_cpu:
+        del pk
     key_gb = be.device_bytes() / 2**30
     # a few distinct seeded witnesses for the same circuit, resident in HBM
     nwit = 4
@@ -371,7 +446,7 @@ def run_b200(args):
         algo_bytes = st["entries"] * (64 + 4) + st["tasks"] * 2 * 128
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         # DRAM bytes per entry from an ncu capture of this kernel at 2^18 (read + write
-        # 439.6 MB over 3,373,063 entries), scaled to this launch's entries
+        # 479.0 MB over 3,932,125 entries), scaled to this launch's entries
         traffic = round(st["entries"] * TRAFFIC_PER_ENTRY) if TRAFFIC_PER_ENTRY else None
         roof = {"bound": "int", "kernel": "k_acc_l1_g1 (G1 bucket accumulation)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),
@@ -394,9 +469,19 @@ def run_b200(args):
 
     # ---- CPU baseline (rank 0, N = 1 only) --------------------------------------
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ms, kind_s, sample = cpu_baseline_reference()
-        cpu = {"value": round(ms, 1), "unit": "ms", "cores": 1, "kind": kind_s, "sample": sample}
+    if want_cpu:
+        g1, g2 = nk.raw_to_arrays(be.prove(wits_host[0]))
+        raw_gpu = np.stack([x[:8] for x in g1]).tobytes() + g2[:16].tobytes()
+        got = cpu_baseline_single(r1, pk, raw_gpu)
+        del pk
+        if got is not None:
+            ms, same = got
+            cpu = {"value": round(ms, 1), "unit": "ms", "cores": 1, "kind": "reference",
+                   "sample": f"one single-threaded reference CPU prove (oracle/_ref: "
+                             f"CpuBackend::prove, backends/cpu/src/backend.cpp:156-201) of the "
+                             f"same {r1.rows}-constraint circuit, key and witness, in its own "
+                             f"process; circuit and key load untimed",
+                   "raw_proof_equal_to_gpu": bool(same)}
 
     if dist is not None:
         dist.barrier()
@@ -408,13 +493,12 @@ def run_b200(args):
         "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)",
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
+        "arith": "Fr and Fq in 8 x 32-bit limbs on the integer pipe; the G1 MSMs' Fq in "
+                 "5 x 52-bit limbs on the FP64 pipe",
         "data": "synthetic (seeded circuit, witness and toxic waste)",
-        "config": {"workload": f"groth16-prove {kind} count={param} density="
-                               f"{['full', 'hybrid', 'sparse'][dens]} ({r1.rows} constraints, "
-                               f"{r1.cols} variables padded)",
-                   "parallelism": f"replicas x{world}", "key_device_gib": round(key_gb, 2),
-                   "l2": "inputs larger than L2 (keys, witness); no flush"},
+        "config": _config(kind, param, dens, r1.rows, r1.cols, world),
+        "key_device_gib": round(key_gb, 2),
         "stages_ms_median": s_med,
         "prepare_ms": {"first": round(prep_ms[0], 1),
                        "tuned": round(statistics.median(prep_ms[1:]), 1)},

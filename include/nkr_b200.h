@@ -244,7 +244,11 @@ int nkr_b200_ntt_device(nkr_b200_ctx *ctx, int op, void *in, void *out, uint64_t
  * array inside the library, shared by all calls on a device: n is limited to
  * 2^16 (larger n returns NKR_B200_EINVAL), and two calls in flight at once on
  * different streams or threads race.  The first call on a device builds the
- * array's tables and waits for `stream`; make it before capturing any stream. */
+ * array's tables and waits for `stream`; make it before capturing any stream.
+ * The set-up belongs to the device's context and runs again after a
+ * cudaDeviceReset.  The array takes 10 MiB of each device the library's kernels
+ * are used on (of every device context it is loaded into when CUDA loads modules
+ * eagerly, CUDA_MODULE_LOADING=EAGER), whether or not this entry point is called. */
 int nkr_b200_ntt_noalloc(int device, int op, const void *in, void *out, uint64_t n,
                          void *stream);
 

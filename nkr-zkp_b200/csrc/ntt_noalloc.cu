@@ -15,13 +15,22 @@
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress, builds the tables in it on the
 // caller's stream and waits for that stream; later calls only enqueue work.  Make
-// the first call on each device before capturing any stream.
+// the first call on each device before capturing any stream.  The address and the
+// tables belong to the device's context: the set-up is keyed by the context's
+// unique id, so after cudaDeviceReset (a new primary context, the module and its
+// array loaded afresh) the next call runs the set-up again.
+//
+// Memory: with lazily loaded modules (CUDA's default) the 10 MiB array is placed
+// on a device when this library's kernels are first used there; with eager
+// loading (CUDA_MODULE_LOADING=EAGER) every context the library is loaded into
+// holds it, whether or not this entry point is called.
 //
 // Sharing: every call on a device uses the same working vector.  Calls ordered on
 // one stream are safe; two calls in flight at once (two streams, or two host
 // threads) overwrite each other's working vector and give wrong results.  No part
 // of the array has to start at zero: the set-up writes every table entry a call
 // reads, and a call writes the working vector before reading it.
+#include <atomic>
 #include <mutex>
 
 #include "ntt.cuh"
@@ -46,13 +55,43 @@ static __device__ __align__(256) uint4 g_ntt_scratch[kScratchFr * 2]; // 2 x 16 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 std::atomic<Fr *> g_base[kMaxDevices];
+std::atomic<unsigned long long> g_ctx_id[kMaxDevices]; // context the tables were built in
 
-// Builds the tables in the array of the current device; returns its Fr base.
-int setup_device(int device, cudaStream_t st, Fr **out)
+// The unique id of the current context (driver cuCtxGetCurrent + cuCtxGetId,
+// reached through the runtime's entry-point query: the library links no libcuda).
+int current_ctx_id(unsigned long long *id)
+{
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    void *ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+        set_error("ntt_noalloc: the current CUDA context could not be identified");
+        return NKR_B200_ECUDA;
+    }
+    return NKR_B200_OK;
+}
+
+// Builds the tables in the array of the current device (context ctx_id); returns
+// its Fr base.
+int setup_device(int device, unsigned long long ctx_id, cudaStream_t st, Fr **out)
 {
     std::lock_guard<std::mutex> lock(g_setup_mu);
     Fr *b = g_base[device].load(std::memory_order_acquire);
-    if (b) {
+    if (b && g_ctx_id[device].load(std::memory_order_acquire) == ctx_id) {
         *out = b;
         return NKR_B200_OK;
     }
@@ -75,6 +114,7 @@ int setup_device(int device, cudaStream_t st, Fr **out)
     NKR_TRY(fr_powers_into(top + kConstGinv, b + kGinvPow, kMax, st));
     for (int lg = 1; lg < kLogMax; ++lg) NKR_TRY(ntt_constants_into(lg, c + 8 * lg, st));
     NKR_CUDA(cudaStreamSynchronize(st));
+    g_ctx_id[device].store(ctx_id, std::memory_order_release);
     g_base[device].store(b, std::memory_order_release);
     *out = b;
     return NKR_B200_OK;
@@ -122,8 +162,11 @@ int ntt_noalloc(int device, int op, const void *in, void *out, uint64_t n, cudaS
     NKR_CUDA(cudaSetDevice(device));
     NKR_TRY(check_device_ptr(in, device, "in"));
     NKR_TRY(check_device_ptr(out, device, "out"));
+    unsigned long long ctx_id = 0;
+    NKR_TRY(current_ctx_id(&ctx_id));
     Fr *b = g_base[device].load(std::memory_order_acquire);
-    if (!b) NKR_TRY(setup_device(device, st, &b));
+    if (!b || g_ctx_id[device].load(std::memory_order_acquire) != ctx_id)
+        NKR_TRY(setup_device(device, ctx_id, st, &b));
     const Fr *c = b + kConsts + 8 * logn;
     Fr *work = b + kWork;
     const Fr *src = static_cast<const Fr *>(in);

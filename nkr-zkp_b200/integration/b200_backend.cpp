@@ -1,6 +1,7 @@
 // Reference-side adapter: registers the B200 prover as an NKR-ZKP Groth16
 // backend.  A maintainer adds this file to the reference as
-// protocols/groth16/backends/b200/src/backend.cpp; it
+// protocols/groth16/backends/b200/src/backend.cpp, with a registry entry and a
+// link target for the accelerator value B200; it
 // implements nkr::groth16::Backend (common/include/groth16/backend.hpp:11-28) on
 // top of the C ABI in include/nkr_b200.h.  It compiles against the reference's
 // own headers (libff types) and is exercised that way by the tests.

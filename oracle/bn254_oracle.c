@@ -597,6 +597,68 @@ int orc_g2_on_curve(const uint64_t *aff)
     return on_curve(2, aff);
 }
 
+/* Fixed-base multiples k_i P of one point (the setup's query points k_i G,
+ * backend.cpp:124-145, where libff uses windowed_exp; any correct method gives
+ * the same canonical affine points): a table T[j][d] = d 2^(8j) P for the 32
+ * byte windows j and digits d, then k_i P = sum_j T[j][byte_j(k_i)]. */
+typedef struct {
+    int d;
+    uint64_t i0, i1;
+    const jac_t *table; /* 32 x 256 */
+    const uint64_t *scalars;
+    uint64_t *out;
+} fixed_job;
+
+static void *fixed_worker(void *arg)
+{
+    fixed_job *J = (fixed_job *)arg;
+    const int d = J->d;
+    for (uint64_t i = J->i0; i < J->i1; ++i) {
+        uint64_t kc[4];
+        from_mont(&FR, J->scalars + 4 * i, kc);
+        jac_t acc;
+        jac_set_inf(d, &acc);
+        for (int j = 0; j < 32; ++j) {
+            const unsigned byte = (unsigned)(kc[j / 8] >> (8 * (j % 8))) & 0xff;
+            if (byte) jac_add(d, &acc, &J->table[256 * j + byte], &acc);
+        }
+        jac_to_aff(d, &acc, J->out + 8 * (uint64_t)d * i);
+    }
+    return NULL;
+}
+
+void orc_fixed_base(int group, const uint64_t *base_aff, const uint64_t *scalars, uint64_t n,
+                    int threads, uint64_t *out_aff)
+{
+    init();
+    const int d = group == 2 ? 2 : 1;
+    if (d == 2) g2_init_b();
+    jac_t *table = (jac_t *)malloc(sizeof(jac_t) * 32 * 256);
+    jac_t step;
+    aff_to_jac(d, base_aff, &step); /* 2^(8j) P */
+    for (int j = 0; j < 32; ++j) {
+        jac_t *row = table + 256 * j;
+        jac_set_inf(d, &row[0]);
+        for (int v = 1; v < 256; ++v) jac_add(d, &row[v - 1], &step, &row[v]);
+        for (int b = 0; b < 8; ++b) jac_dbl(d, &step, &step);
+    }
+    if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads > 64) threads = 64;
+    if ((uint64_t)threads > n) threads = n ? (int)n : 1;
+    pthread_t tid[64];
+    fixed_job jobs[64];
+    for (int t = 0; t < threads; ++t) {
+        jobs[t] = (fixed_job){d, n * t / threads, n * (t + 1) / threads, table, scalars, out_aff};
+        if (threads == 1)
+            fixed_worker(&jobs[t]);
+        else
+            pthread_create(&tid[t], NULL, fixed_worker, &jobs[t]);
+    }
+    if (threads > 1)
+        for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+    free(table);
+}
+
 /* ------------------------------------------------------------------------- */
 /* radix-2 domain (libfqfft basic_radix2_domain)                              */
 /* ------------------------------------------------------------------------- */

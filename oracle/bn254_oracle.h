@@ -54,6 +54,10 @@ void orc_g1_generator(uint64_t *aff);
 void orc_g2_generator(uint64_t *aff);
 int orc_g1_on_curve(const uint64_t *aff);
 int orc_g2_on_curve(const uint64_t *aff);
+/* k_i P for n scalars (Fr Montgomery) and one affine base P of group 1 or 2;
+ * results affine (64 / 128 B each).  threads <= 0 -> all cores. */
+void orc_fixed_base(int group, const uint64_t *base_aff, const uint64_t *scalars, uint64_t n,
+                    int threads, uint64_t *out_aff);
 
 /* Multi-scalar multiplication: bases are AFFINE (64 / 128 B) in libff encoding,
  * scalars Fr Montgomery; result affine.  threads <= 0 -> all cores. */

@@ -16,6 +16,7 @@ import ctypes
 import hashlib
 import os
 import struct
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -168,6 +169,15 @@ class Oracle:
         f(_p(_arr(bases_aff)), _p(s), _U64(s.size // 4), ctypes.c_int(threads), _p(out))
         return out
 
+    def fixed_base(self, group, base_aff, scalars, threads=0):
+        """k_i * P for every scalar k_i (Fr Montgomery), affine (8 / 16 u64 per point)."""
+        s = _arr(scalars)
+        n = s.size // 4
+        out = np.zeros((n, 8 * group), np.uint64)
+        self.lib.orc_fixed_base(ctypes.c_int(group), _p(_arr(base_aff)), _p(s), _U64(n),
+                                ctypes.c_int(threads), _p(out))
+        return out
+
     def quotient(self, az, bz, cz):
         n = _arr(az).size // 4
         a, b, c = _arr(az).copy(), _arr(bz).copy(), _arr(cz).copy()
@@ -246,6 +256,7 @@ class Ref:
         self.lib.ref_prover_open.restype = _VP
         self.lib.ref_prover_open.argtypes = [_VP, ctypes.c_char_p]
         self.lib.ref_prover_prove.argtypes = [_VP, _VP, _VP, _VP]
+        self.lib.ref_prover_prove_blind.argtypes = [_VP, _VP, _VP, _VP, _VP]
         self.lib.ref_prover_close.argtypes = [_VP]
         assert self.lib.ref_init() == 0
 
@@ -331,6 +342,35 @@ class Ref:
 
     def prover_close(self, h):
         self.lib.ref_prover_close(h)
+
+    def prover_prove_blind(self, h, witness):
+        """groth16.prove.total of the reference CLI: prove, then blind_proof with the
+        reference's own random r, s.  Returns (a, b, c) affine in Jacobian layout."""
+        a, b, c = np.zeros(12, np.uint64), np.zeros(24, np.uint64), np.zeros(12, np.uint64)
+        self._ok(self.lib.ref_prover_prove_blind(h, _p(_arr(witness)), _p(a), _p(b), _p(c)),
+                 "prover_prove_blind")
+        return a, b, c
+
+    def quotient_vectors(self, r1cs, witness):
+        """az, bz, cz and H of the CPU backend's prove (reference libff / libfqfft)."""
+        c = self._circuit(r1cs)
+        outs = [np.zeros((r1cs.rows, 4), np.uint64) for _ in range(4)]
+        self._ok(self.lib.ref_quotient_vectors(ctypes.byref(c), _p(_arr(witness)),
+                                               *[_p(o) for o in outs]), "quotient_vectors")
+        return outs
+
+    def seeded_pairs(self, count, density, seed):
+        """The Poseidon preimages the repository's seeded generator draws (2 count Fr)."""
+        out = np.zeros((2 * count, 4), np.uint64)
+        self._ok(self.lib.ref_seeded_pairs(_U64(count), ctypes.c_int(density), _U64(seed), _p(out)),
+                 "seeded_pairs")
+        return out
+
+    def poseidon_circuit_seeded(self, count, density, seed):
+        """generate("poseidon", count, density, seed) built by the reference's own
+        Poseidon gadget and R1CSManager (no part of this repository's library)."""
+        d = self.poseidon_circuit_n(self.seeded_pairs(count, density, seed))
+        return SimpleNamespace(**d)
 
     def verify(self, vk_path, public_inputs, proof_path):
         ok = ctypes.c_int()

@@ -11,10 +11,13 @@
 // writes): Fr/Fq = 4 x u64 little-endian Montgomery limbs; G1 = {X,Y,Z} Fq
 // Jacobian (96 B); G2 = {X,Y,Z} Fq2 with Fq2 = {c0,c1} (192 B).
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <exception>
 #include <map>
+#include <random>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -306,6 +309,115 @@ int ref_prover_prove(void *h, const void *witness, void *g1_out4, void *g2_out)
 }
 
 void ref_prover_close(void *h) { delete static_cast<RefProver *>(h); }
+
+// What groth16-prove times as groth16.prove.total (app/prove.cpp:70-88): the CPU
+// backend's prove, then the reference's blind_proof (protocol.cpp:85-94) with
+// its own unseeded r, s.  Writes the proof affine-normalised in libff's Jacobian
+// layout (Z = 1): a (96 B), b (192 B), c (96 B).
+int ref_prover_prove_blind(void *h, const void *witness, void *a_out, void *b_out, void *c_out)
+{
+    REF_TRY({
+        auto *p = static_cast<RefProver *>(h);
+        auto w = from_raw<Scalar>(witness, p->circuit.a.num_cols);
+        auto backend = make_cpu_backend();
+        RawProof raw;
+        backend->prove(p->circuit, p->pk, w, raw);
+        const Proof proof = blind_proof(p->pk, raw);
+        write_affine(proof.a, a_out);
+        write_affine(proof.b, b_out);
+        write_affine(proof.c, c_out);
+    })
+}
+
+// The SpMV vectors and the quotient H of the CPU backend's prove
+// (backends/cpu/src/backend.cpp:163-179) on the reference's own libff / libfqfft
+// types.  backend.cpp keeps its `multiply` (lines 25-35) file-local, so the row
+// loop below repeats it: per row, value += values[j] * z[col_idx[j]] in CSR order.
+int ref_quotient_vectors(const RawCircuit *rc, const void *witness, void *az_out, void *bz_out,
+                         void *cz_out, void *h_out)
+{
+    REF_TRY({
+        Circuit c = circuit_from_raw(*rc);
+        auto z = from_raw<Scalar>(witness, rc->cols);
+        auto multiply = [&](const CsrMatrix<Scalar> &m) {
+            std::vector<Scalar> out(m.num_rows, Scalar::zero());
+            for (std::size_t row = 0; row < m.num_rows; ++row) {
+                Scalar value = Scalar::zero();
+                for (std::size_t j = m.row_ptr[row]; j < m.row_ptr[row + 1]; ++j)
+                    value += m.values[j] * z[m.col_idx[j]];
+                out[row] = value;
+            }
+            return out;
+        };
+        const std::size_t rows = c.constraints();
+        auto domain = libfqfft::get_evaluation_domain<Scalar>(rows);
+        if (!domain || domain->m != rows) throw std::invalid_argument("unsupported R1CS domain size");
+        std::vector<Scalar> az = multiply(c.a), bz = multiply(c.b), cz = multiply(c.c);
+        std::memcpy(az_out, az.data(), rows * 32);
+        std::memcpy(bz_out, bz.data(), rows * 32);
+        std::memcpy(cz_out, cz.data(), rows * 32);
+        domain->iFFT(az);
+        domain->iFFT(bz);
+        domain->iFFT(cz);
+        const Scalar coset = Scalar::multiplicative_generator;
+        domain->cosetFFT(az, coset);
+        domain->cosetFFT(bz, coset);
+        domain->cosetFFT(cz, coset);
+        for (std::size_t i = 0; i < rows; ++i) az[i] = az[i] * bz[i] - cz[i];
+        domain->divide_by_Z_on_coset(az);
+        domain->icosetFFT(az, coset);
+        std::memcpy(h_out, az.data(), rows * 32);
+    })
+}
+
+// The Poseidon preimages (left, right per hash; 2 * count Fr, Montgomery limbs)
+// that this repository's seeded circuit generator draws for
+// generate("poseidon", count, density, seed), so that the reference's own
+// builders (ref_poseidon_circuit_n) can build the same circuit without it.  The
+// reference's generator draws the same distribution from unseeded engines
+// (common/include/density.hpp:62,80-98): ceil(N/10) nonzero at sparse density,
+// N - N/2 at hybrid, all at full.  One std::mt19937_64(seed) drives every draw:
+// a mask with the zeros at its end, shuffled by Fisher-Yates (j = rng() % i for
+// i = N down to 2), then, slot by slot, a nonzero uniform Fr for each set bit
+// (four 64-bit words, the top one cut to 62 bits, values >= r and zero redrawn).
+int ref_seeded_pairs(uint64_t count, int density, uint64_t seed, void *lr_out)
+{
+    REF_TRY({
+        const uint64_t n = 2 * count;
+        uint64_t nonzero;
+        switch (density) {
+        case 0: nonzero = n; break;
+        case 1: nonzero = n - n / 2; break;
+        case 2: nonzero = n / 10 + (n % 10 != 0); break;
+        default: throw std::invalid_argument("density must be 0, 1 or 2");
+        }
+        std::mt19937_64 rng(seed);
+        std::vector<uint8_t> mask(n, 1);
+        std::fill(mask.end() - (n - nonzero), mask.end(), 0);
+        for (uint64_t i = n; i > 1; --i) std::swap(mask[i - 1], mask[rng() % i]);
+        static const uint64_t kR[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull,
+                                       0xb85045b68181585dull, 0x30644e72e131a029ull};
+        auto below_r = [](const uint64_t v[4]) {
+            for (int i = 3; i >= 0; --i)
+                if (v[i] != kR[i]) return v[i] < kR[i];
+            return false;
+        };
+        uint64_t *out = static_cast<uint64_t *>(lr_out);
+        for (uint64_t i = 0; i < n; ++i) {
+            uint64_t *v = out + 4 * i;
+            if (!mask[i]) {
+                v[0] = v[1] = v[2] = v[3] = 0;
+                continue;
+            }
+            do {
+                do {
+                    for (int k = 0; k < 4; ++k) v[k] = rng();
+                    v[3] &= (uint64_t(1) << 62) - 1;
+                } while (!below_r(v));
+            } while (!(v[0] | v[1] | v[2] | v[3]));
+        }
+    })
+}
 
 // The reference CPU setup (backend.cpp:41-154); unseeded toxic waste as in the
 // reference.  Writes the reference's .pk.bin / .vk.bin artifacts.

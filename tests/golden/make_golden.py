@@ -3,7 +3,7 @@
 Run in a checkout where the reference source tree is present and
 oracle/_ref/libnkr_ref.so has been built from it (`make -C oracle ref`):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference source tree>   (or NKR_REFERENCE_SRC)
 
 Everything here is computed by the reference's own code (libff, libfqfft, the
 groth16 CPU backend and setup, its Poseidon helper) through oracle/_ref, except
@@ -32,7 +32,9 @@ sys.path.insert(0, os.path.join(ROOT, "nkr-zkp_b200"))
 import oracle as O  # noqa: E402
 
 GOLD = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF_SRC = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NKR_REFERENCE_SRC")
+if not REF_SRC:
+    sys.exit("usage: make_golden.py <reference source tree> (or set NKR_REFERENCE_SRC)")
 
 
 def hexs(a):

@@ -29,6 +29,16 @@ def test_domain_ops_golden(ctx):
         assert O.sha256_arr(ctx.ntt(int(op), x)) == digest, f"op {op}"
 
 
+@pytest.mark.parametrize("logn", [20, 24])
+def test_full_vectors_match_oracle_at_benchmark_sizes(ctx, orc, logn, rng):
+    """Every output element against the oracle's serial libfqfft restatement:
+    all five domain ops at 2^20 (the prove's domain), the FFT at 2^24."""
+    n = 1 << logn
+    x = O.random_fr(n, rng)
+    for op in (range(5) if logn == 20 else (0,)):
+        assert np.array_equal(ctx.ntt(op, x), orc.domain_op(op, x)), f"op {op} n 2^{logn}"
+
+
 @pytest.mark.parametrize("logn", [20, 22, 24])
 def test_large_round_trips_and_spot_values(ctx, logn, rng):
     """Size-independent properties at the benchmark sizes: inverse pairs are

@@ -145,3 +145,57 @@ def test_blind_then_reference_verify(orc, ref, tmp_path):
     c2 = orc.add_affine(1, c, orc.g1_generator())
     O.write_proof(path, O.affine_to_jac(1, a), O.affine_to_jac(2, b), O.affine_to_jac(1, c2))
     assert not ref.verify(os.path.join(GOLDEN, "matmul4.vk.bin"), pub, path)
+
+
+def test_fixed_base_equals_reference_multiples(orc, ref):
+    """The oracle's fixed-base multiples (the key generator of the 2^20 golden
+    fixture) equal libff's k * G on both groups, edge scalars included."""
+    rng = np.random.default_rng(31)
+    ks = O.random_fr(24, rng)
+    ks[0] = 0
+    ks[1] = O.fr_mont(1)
+    ks[2] = O.fr_mont(O.R - 1)
+    ks[3] = O.fr_mont(2**255 % O.R)
+    for group, gen in ((1, orc.g1_generator()), (2, orc.g2_generator())):
+        got = orc.fixed_base(group, gen, ks, threads=3)
+        for i in range(ks.shape[0]):
+            assert np.array_equal(got[i], ref.mul_gen(group, ks[i])[:8 * group]), (group, i)
+
+
+@pytest.mark.parametrize("count,dens,seed", [(1, 0, 2), (4, 2, 3), (9, 1, 7)])
+def test_reference_builder_reproduces_seeded_circuit(ref, count, dens, seed):
+    """The reference's own Poseidon gadget fed with the seeded preimages builds the
+    generator's circuit and witness entry for entry (how the benchmark's reference
+    arm gets the workload without this repository's library)."""
+    import nkr_b200 as nk
+    mine = nk.generate("poseidon", count, dens, seed=seed)
+    theirs = ref.poseidon_circuit_seeded(count, dens, seed)
+    assert (mine.rows, mine.cols, mine.public_inputs) == (theirs.rows, theirs.cols, theirs.public_inputs)
+    for k in range(3):
+        assert np.array_equal(mine.row_ptr[k], theirs.row_ptr[k])
+        assert np.array_equal(mine.col_idx[k], theirs.col_idx[k])
+        assert np.array_equal(mine.values[k], theirs.values[k])
+    assert np.array_equal(mine.witness, theirs.witness)
+
+
+def test_reference_quotient_vectors_equal_oracle(orc, ref):
+    c = ref.poseidon_circuit_seeded(3, 2, 5)
+    az, bz, cz, h = ref.quotient_vectors(c, c.witness)
+    for k, v in enumerate((az, bz, cz)):
+        assert np.array_equal(v, orc.spmv(c.rows, c.row_ptr[k], c.col_idx[k], c.values[k], c.witness))
+    assert np.array_equal(h, orc.quotient(az, bz, cz))
+
+
+def test_golden_2_20_fixture_is_consistent():
+    """The 2^20 fixture names the generator's circuit and holds every digest the
+    GPU test compares (the GPU test itself runs with -m gpu)."""
+    import nkr_b200 as nk
+    g = json.load(open(os.path.join(GOLDEN, "prove_poseidon2048.json")))
+    assert g["reference_verifier_accepts"]
+    c = g["circuit"]
+    assert (c["rows"], c["cols"]) == (1 << 20, 1 << 20)
+    assert set(g["raw"]) == {"ar", "bs1", "zk", "qz", "bs2"}
+    assert set(g["vectors"]) == {"az", "bz", "cz", "h"}
+    assert set(g["proof"]) == {"a", "b", "c"}
+    r1 = nk.generate(c["kind"], c["count"], c["density"], seed=c["seed"])
+    assert O.sha256_arr(r1.witness) == c["witness"]
