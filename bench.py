@@ -54,10 +54,21 @@ METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
 # DRAM read + write bytes per (point, digit) entry of the G1 accumulation kernel,
 # from an ncu capture at 2^18 points (a 2^20 capture would hold ~6 GB of keys on
 # the device); traffic grows with entries (one random base gather per entry)
-TRAFFIC_PER_ENTRY = (452.237056e6 + 26.803968e6) / 3932125   # 121.8 B per entry
+TRAFFIC_PER_ENTRY = (449.213184e6 + 22.324480e6) / 3932125   # 119.9 B per entry
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_acc_l1_g1 on the "
-                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 121.8 B "
+                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 119.9 B "
                   "per entry, scaled by this launch's entries")
+# Thread instructions per 52-bit-limb Fq product: ncu smsp__inst_executed.sum x 32 over
+# the products of nkr_b200_bench_mul's FP64 form (7,027,636,736 warp instructions for
+# 148 x 16 x 256 threads x 256 x 4 = 620,756,992 products).
+INSTR_PER_PRODUCT = 7027636736 * 32 / 620756992   # 362.3
+# Pipe counters of k_acc_l1_g1 from one ncu launch (2^18-point uniform G1 MSM of
+# --mode kernels; profiles/k_acc_l1_g1_msm_2_18.md); percentages of peak.
+ACC_NCU = {"issue_active_pct": 59.34, "fp64_pipe_pct": 40.79, "alu_pipe_pct": 52.55,
+           "fmaheavy_pipe_pct": 22.86, "warps_active_per_sm": 10.67, "registers": 168,
+           "stall_per_issue": {"wait": 0.83, "not_selected": 0.76, "math_pipe_throttle": 0.63,
+                               "long_scoreboard": 0.57},
+           "source": "ncu --metrics ... -k regex:k_acc_l1_g1 -c 1, --clock-control none"}
 
 
 def _dist():
@@ -424,12 +435,17 @@ def run_b200(args):
 
     # ---- roofline of the dominant kernel (MSM bucket accumulation) ---------------
     peaks = _measured_peaks()
-    # the denominator is the fastest Fq product this GPU sustains in registers: the
-    # integer-pipe CIOS (variant 0) and the FP64-pipe 52-bit-limb product (variant 3,
-    # the one the G1 accumulation runs on); the larger one is the roof
+    # The product roof is the instruction-issue ceiling of the 52-bit-limb Fq product
+    # the G1 accumulation runs: every SM issues 4 warp instructions per cycle and one
+    # product costs INSTR_PER_PRODUCT thread instructions (ncu), so no kernel built
+    # from these products exceeds SMs x 4 x 32 x f_sm / INSTR_PER_PRODUCT products/s.
+    # The best register-resident microbenchmark of the same product (itself at ~58%
+    # issue) is reported beside it.
     peak_int, _ = ctx.bench_mul(1)
     peak_fp64, _ = ctx.bench_mul(1 | (3 << 8))
-    muls_peak = max(peak_int, peak_fp64)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    f_sm = (clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0) * 1e6
+    issue_peak = sms * 4 * 32 * f_sm / INSTR_PER_PRODUCT
     mb = nk.MsmBases(ctx, 1, be._keep["a_query"]) if hasattr(be, "_keep") and be._keep else None
     roof = None
     if mb is not None:
@@ -445,16 +461,23 @@ def run_b200(args):
         # plus the task bucket ids and bucket / partial writes (128 B each)
         algo_bytes = st["entries"] * (64 + 4) + st["tasks"] * 2 * 128
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        # DRAM bytes per entry from an ncu capture of this kernel at 2^18 (read + write
-        # 479.0 MB over 3,932,125 entries), scaled to this launch's entries
+        # DRAM bytes per entry from an ncu capture of this kernel at 2^18, scaled to
+        # this launch's entries
         traffic = round(st["entries"] * TRAFFIC_PER_ENTRY) if TRAFFIC_PER_ENTRY else None
         roof = {"bound": "int", "kernel": "k_acc_l1_g1 (G1 bucket accumulation)",
-                "achieved": round(achieved / 1e9, 2), "peak": round(muls_peak / 1e9, 2),
-                "unit": "G Fq-mul/s", "frac": round(achieved / muls_peak, 3),
-                "peak_source": "measured: nkr_b200_bench_mul register-resident Fq Montgomery "
-                               "products, best formulation (MEASURED_PEAKS.json has no integer peak)",
-                "peak_by_pipe": {"int_cios": round(peak_int / 1e9, 2),
-                                 "fp64_52bit": round(peak_fp64 / 1e9, 2)},
+                "achieved": round(achieved / 1e9, 2), "peak": round(issue_peak / 1e9, 2),
+                "unit": "G Fq-mul/s", "frac": round(achieved / issue_peak, 3),
+                "peak_source": f"instruction-issue ceiling of the FP64-limb Fq product: {sms} SMs "
+                               f"x 4 warp instructions/cycle x 32 x {f_sm / 1e6:.0f} MHz (SM clock "
+                               f"sampled in the timed region) / {INSTR_PER_PRODUCT:.1f} instructions "
+                               f"per product (ncu on nkr_b200_bench_mul); no FLOP or integer peak "
+                               f"in MEASURED_PEAKS.json applies",
+                "microbench": {"int_cios": round(peak_int / 1e9, 2),
+                               "fp64_52bit": round(peak_fp64 / 1e9, 2),
+                               "frac_of_best": round(achieved / max(peak_int, peak_fp64), 3),
+                               "note": "register-resident product chains (nkr_b200_bench_mul), "
+                                       "issue active ~58% themselves"},
+                "ncu": ACC_NCU,
                 "units_per_launch": {"entries": st["entries"], "fq_muls": muls,
                                      "window_bits": st["window_bits"], "windows": st["windows"],
                                      "buckets": st["buckets"]},
@@ -664,14 +687,19 @@ def run_serve(args):
         be.prove(None, witness_ptr=ws[0].data_ptr())
         service.append(time.perf_counter() - t)
     mean_s = sum(service) / len(service)
-    lam = args.serve_load / mean_s  # offered load as a fraction of the plain path's capacity
-    rng = np.random.default_rng(5)
     n_req = args.serve_requests
-    arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
-    which = rng.integers(0, len(keys), n_req)
-    wsel = [int(rng.integers(0, len(wits[k]))) for k in which]
 
-    def replay(submit, wait_all):
+    def stream(load, seed):
+        """Poisson arrivals at `load` x the plain path's capacity (one request per
+        mean plain service time at load 1), keys uniform, seeded."""
+        rng = np.random.default_rng(seed)
+        lam = load / mean_s
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
+        which = rng.integers(0, len(keys), n_req)
+        wsel = [int(rng.integers(0, len(wits[k]))) for k in which]
+        return lam, arrivals, which, wsel
+
+    def replay(arrivals, submit, wait_all):
         t0 = time.perf_counter()
         handles = []
         for i in range(n_req):
@@ -683,7 +711,7 @@ def run_serve(args):
         return res, time.perf_counter() - t0
 
     # plain arm: one request at a time in arrival order (FIFO), the same arrivals
-    def plain_arm():
+    def plain_arm(arrivals, which, wsel):
         done = [None] * n_req
         q, cv = [], threading.Condition()
 
@@ -704,11 +732,12 @@ def run_serve(args):
                 q.append((i, t0))
                 cv.notify()
             return i
-        res, wall = replay(submit, lambda h: (th.join(), done)[1])
+        res, wall = replay(arrivals, submit, lambda h: (th.join(), done)[1])
         return res, wall
 
-    def server_arm():
+    def server_arm(arrivals, which, wsel, ageing):
         sv = nk.Server(ctx, max_inflight=args.serve_inflight, max_slots_per_key=4)
+        sv.set_ageing(ageing)
         ids = [sv.add_key(be) for be in bes]
 
         def submit(i, t0):
@@ -721,10 +750,11 @@ def run_serve(args):
                 raw, lat, _ = sv.wait(h)
                 out.append((bytes(raw), lat))
             return out
-        res, wall = replay(submit, wait_all)
+        res, wall = replay(arrivals, submit, wait_all)
         slots = [sv.slots(i) for i in ids]
+        aged = sv.stats()["aged"]
         sv.close()
-        return res, wall, slots
+        return res, wall, slots, aged
 
     clocks = ClockSampler(0)
     # server warm-up: slots and graphs of every key
@@ -738,28 +768,47 @@ def run_serve(args):
     server_arm_warm.close()
     clocks.start()
     launches0 = nk.launch_count()
-    plain, plain_wall = plain_arm()
-    srv, srv_wall, slots = server_arm()
+    ok = True
+
+    def summary(res, wall):
+        lat = [x[1] for x in res]
+        return {"proofs_per_s": round(n_req / wall, 2), "p50_ms": round(_percentile(lat, 50), 2),
+                "p99_ms": round(_percentile(lat, 99), 2)}
+
+    def exact(res, which, wsel):
+        return all(res[i][0] == expect[which[i]][wsel[i]] for i in range(n_req))
+
+    # the offered load below capacity: latency; the server with and without ageing
+    lam, arrivals, which, wsel = stream(args.serve_load, 5)
+    plain, plain_wall = plain_arm(arrivals, which, wsel)
+    srv, srv_wall, slots, aged = server_arm(arrivals, which, wsel, args.serve_age)
+    srv0, srv0_wall, _, _ = server_arm(arrivals, which, wsel, 0.0)
+    ok = ok and exact(plain, which, wsel) and exact(srv, which, wsel) and exact(srv0, which, wsel)
+    # saturation: offered load above the plain path's capacity, so each arm runs
+    # at its own throughput
+    lam_sat, arr_s, which_s, wsel_s = stream(args.serve_sat_load, 6)
+    plain_s, plain_s_wall = plain_arm(arr_s, which_s, wsel_s)
+    srv_s, srv_s_wall, _, aged_s = server_arm(arr_s, which_s, wsel_s, args.serve_age)
+    ok = ok and exact(plain_s, which_s, wsel_s) and exact(srv_s, which_s, wsel_s)
     clk = clocks.stop()
-    ok = all(plain[i][0] == expect[which[i]][wsel[i]] and srv[i][0] == expect[which[i]][wsel[i]]
-             for i in range(n_req))
-    lat_p = [x[1] for x in plain]
-    lat_s = [x[1] for x in srv]
     line = {
         "metric": "served Groth16 proofs/s and latency, Poisson stream over 6 resident keys",
-        "value": round(n_req / srv_wall, 2), "unit": "proofs/s", "n_gpus": 1,
-        "higher_is_better": True, "dtype": "bn254 (exact modular; u32 limbs, G1 MSM in 52-bit FP64 limbs)", "bit_exact": ok,
+        "value": round(n_req / srv_s_wall, 2), "unit": "proofs/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": DTYPE, "bit_exact": ok,
         "data": "synthetic (seeded circuits, witnesses, toxic waste and arrivals)",
         "config": {"workload": "keys " + ", ".join(f"{k} {p}" for k, p, _ in keys),
-                   "requests": n_req, "offered_load": args.serve_load,
-                   "arrival_rate_per_s": round(lam, 2),
+                   "requests_per_arm": n_req,
                    "plain_service_ms": [round(x * 1e3, 2) for x in service],
-                   "max_inflight": args.serve_inflight, "slots_used": slots},
-        "server": {"proofs_per_s": round(n_req / srv_wall, 2),
-                   "p50_ms": round(_percentile(lat_s, 50), 2), "p99_ms": round(_percentile(lat_s, 99), 2)},
-        "plain_fifo": {"proofs_per_s": round(n_req / plain_wall, 2),
-                       "p50_ms": round(_percentile(lat_p, 50), 2),
-                       "p99_ms": round(_percentile(lat_p, 99), 2)},
+                   "max_inflight": args.serve_inflight, "slots_used": slots,
+                   "ageing_factor": args.serve_age},
+        "saturation": {"offered_load": args.serve_sat_load, "arrival_rate_per_s": round(lam_sat, 2),
+                       "server": dict(summary(srv_s, srv_s_wall), aged=aged_s),
+                       "plain_fifo": summary(plain_s, plain_s_wall),
+                       "speedup_vs_plain": round(plain_s_wall / srv_s_wall, 3)},
+        "below_capacity": {"offered_load": args.serve_load, "arrival_rate_per_s": round(lam, 2),
+                           "server": dict(summary(srv, srv_wall), aged=aged),
+                           "server_no_ageing": summary(srv0, srv0_wall),
+                           "plain_fifo": summary(plain, plain_wall)},
         "gpu_launches": nk.launch_count() - launches0, "clocks": clk, "setup_s": round(setup_s, 1),
         "key_device_gib": round(sum(be.device_bytes() for be in bes) / 2**30, 2),
     }
@@ -1068,6 +1117,8 @@ def main():
     ap.add_argument("--serve-keys", type=int, default=6)
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--serve-sat-load", type=float, default=1.5)
+    ap.add_argument("--serve-age", type=float, default=1.0)
     ap.add_argument("--serve-inflight", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -96,9 +96,14 @@ typedef struct {
 
 /* Per-stage device times of the last prove on a key, milliseconds (CUDA events):
  * the reference's profile labels groth16.cuda.prove.{r1cs_matrix_vector,
- * quotient_polynomial, witness_msms, quotient_msm} (groth16_backend.cu:249-274). */
+ * quotient_polynomial, witness_msms, quotient_msm} (groth16_backend.cu:249-274).
+ * The stages overlap on the device (the witness MSMs run on their own streams
+ * beside the quotient chain), so each MSM's end is also given, measured from the
+ * start of the prove: the labels groth16.cpu.prove.msm_{a, b_g1, b_g2, l, h} of
+ * the CPU backend (backends/cpu/src/backend.cpp:181-200). */
 typedef struct {
     float spmv_ms, quotient_ms, witness_msms_ms, quotient_msm_ms, total_ms;
+    float msm_a_end_ms, msm_b_g1_end_ms, msm_b_g2_end_ms, msm_l_end_ms, msm_h_end_ms;
 } nkr_b200_stage_times;
 
 /* ---- context -------------------------------------------------------------- */
@@ -199,9 +204,11 @@ int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses
  * fill the GPU alone -- and max_inflight in total) and replays each slot's
  * captured prove graph, so requests of different circuits overlap on the GPU.
  * Slot streams take a priority by circuit size, so the GPU's block scheduler
- * serves the smaller proofs in flight first (low median latency; the largest
- * circuit's requests absorb the wait).  The witness memory of a request must
- * stay valid until its wait returns.
+ * serves the smaller proofs in flight first (low median latency).  Requests
+ * age: one that waited longer than age_factor (default 1) times its key's
+ * recent service time is launched at the device's highest stream priority, so
+ * the largest circuit's requests do not absorb all of the small ones' priority.
+ * The witness memory of a request must stay valid until its wait returns.
  * A key added to a server is proved only through that server while it runs. */
 typedef struct nkr_b200_server nkr_b200_server;
 int nkr_b200_server_create(nkr_b200_ctx *ctx, int max_inflight, int max_slots_per_key,
@@ -214,6 +221,12 @@ int nkr_b200_server_submit(nkr_b200_server *server, int key_id, const void *witn
 int nkr_b200_server_wait(nkr_b200_server *server, uint64_t request_id, nkr_b200_raw_proof *out,
                          double *latency_ms, double *queue_ms);
 int nkr_b200_server_slots(nkr_b200_server *server, int key_id, int *slots);
+/* Ageing threshold as a multiple of a key's recent service time (0 turns ageing
+ * off); applies to requests started after the call. */
+int nkr_b200_server_set_ageing(nkr_b200_server *server, double age_factor);
+/* Requests completed, failed, and launched aged (at the highest priority) so far. */
+int nkr_b200_server_stats(nkr_b200_server *server, uint64_t *completed, uint64_t *failed,
+                          uint64_t *aged);
 void nkr_b200_server_destroy(nkr_b200_server *server);
 
 /* ---- operator-level entry points (operators/cuda/include/nkr/operators/cuda.hpp) */
@@ -234,6 +247,25 @@ int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n);
  * is non-NULL, in which case the call waits and returns the ops' device time. */
 int nkr_b200_ntt_device(nkr_b200_ctx *ctx, int op, void *in, void *out, uint64_t n, void *stream,
                         float *device_ms);
+
+/* The constants that define this library's domain of size n (a power of two):
+ * omega, the n-th root of unity libfqfft's radix-2 domain uses
+ * (get_root_of_unity, libfqfft field_utils.tcc:38-51), and coset, the
+ * multiplicative generator 5 (alt_bn128_init.cpp:59), both Fr Montgomery
+ * (32 B).  NTTContext is constructed with these two values
+ * (backends/cuda/src/groth16_backend.cu:87, ntt/ntt.cuh:52); the operator
+ * layer in nkr_b200_operators.hpp checks what its caller passes against them. */
+int nkr_b200_domain_constants(nkr_b200_ctx *ctx, uint64_t n, void *omega, void *coset);
+
+/* The pointwise step of the quotient on device vectors of the domain's size n:
+ * out[i] = (a[i] b[i] - c[i]) (g^n - 1)^-1 with the coset generator g = 5, what
+ * NTTContext::A_times_B_minus_C_divided_by_Z (ntt/ntt.cuh:187-207) computes into
+ * its first argument (with one field inverse for the whole call instead of one
+ * per element).  Element-wise, so out may be a, b or c.  Enqueued on stream
+ * (NULL = the legacy default stream); the first call for a size builds that
+ * size's tables. */
+int nkr_b200_quotient_device(nkr_b200_ctx *ctx, const void *a, const void *b, const void *c,
+                             void *out, uint64_t n, void *stream);
 
 /* The same five domain ops on DEVICE buffers, allocating no device memory.  No
  * counterpart in the reference: it serves callers that cannot allocate (their own

@@ -37,18 +37,25 @@ const char *get_error() { return g_err; }
 
 int device_alloc(void **p, size_t bytes, const char *what)
 {
-    size_t free_b = 0, total_b = 0;
-    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
-    if (e != cudaSuccess) {
-        set_error("cudaMemGetInfo: %s", cudaGetErrorString(e));
-        return NKR_B200_ECUDA;
-    }
-    // keep 512 MiB of headroom for the runtime and other tenants of the GPU
-    const size_t reserve = size_t(512) << 20;
-    if (bytes + reserve > free_b) {
-        set_error("device memory admission refused for %s: need %zu B, %zu B free", what, bytes,
-                  free_b);
-        return NKR_B200_ENOMEM;
+    // Admission against free HBM for large buffers, keeping 512 MiB of headroom for
+    // the runtime and other tenants of the GPU.  Buffers under 64 MiB skip the
+    // query (cudaMemGetInfo costs about as much as the allocation itself, and a
+    // small key's prove slot makes ~90 of them): a failing cudaMalloc still
+    // reports NKR_B200_ENOMEM.
+    cudaError_t e;
+    if (bytes >= (size_t(64) << 20)) {
+        size_t free_b = 0, total_b = 0;
+        e = cudaMemGetInfo(&free_b, &total_b);
+        if (e != cudaSuccess) {
+            set_error("cudaMemGetInfo: %s", cudaGetErrorString(e));
+            return NKR_B200_ECUDA;
+        }
+        const size_t reserve = size_t(512) << 20;
+        if (bytes + reserve > free_b) {
+            set_error("device memory admission refused for %s: need %zu B, %zu B free", what, bytes,
+                      free_b);
+            return NKR_B200_ENOMEM;
+        }
     }
     e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
@@ -315,6 +322,48 @@ int nkr_b200_ntt_device(nkr_b200_ctx *ctx, int op, void *in, void *out, uint64_t
         cudaEventDestroy(e1);
     }
     return NKR_B200_OK;
+}
+
+int nkr_b200_domain_constants(nkr_b200_ctx *ctx, uint64_t n, void *omega, void *coset)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(omega && coset, "null output");
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "domain size %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)n);
+    const NttTables *T;
+    NKR_TRY(get_tables(ctx, logn, &T));
+    Fr c[kConstGinv + 1];
+    NKR_CUDA(cudaMemcpyAsync(c, T->consts.p, sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
+    NKR_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(omega, &c[kConstOmega], 32);
+    std::memcpy(coset, &c[kConstG], 32);
+    return NKR_B200_OK;
+}
+
+int nkr_b200_quotient_device(nkr_b200_ctx *ctx, const void *a, const void *b, const void *c,
+                             void *out, uint64_t n, void *stream)
+{
+    NKR_TRY(ctx_check(ctx));
+    NKR_REQUIRE(a && b && c && out, "null data");
+    const int logn = log2_exact(n);
+    NKR_REQUIRE(logn >= 1 && logn <= 28, "quotient size %llu must be a power of two in [2, 2^28]",
+                (unsigned long long)n);
+    for (const void *p : {a, b, c, static_cast<const void *>(out)}) {
+        cudaPointerAttributes attr{};
+        const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+        if (e != cudaSuccess) cudaGetLastError();
+        NKR_REQUIRE(e == cudaSuccess && attr.type == cudaMemoryTypeDevice &&
+                        attr.device == ctx->device,
+                    "quotient buffers must be device memory of device %d", ctx->device);
+    }
+    const NttTables *T;
+    NKR_TRY(get_tables(ctx, logn, &T));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    // element-wise: out may be a, b or c
+    return fr_quotient_pointwise(static_cast<const Fr *>(a), static_cast<const Fr *>(b),
+                                 static_cast<const Fr *>(c), static_cast<Fr *>(out), n,
+                                 T->consts.as<Fr>() + kConstZinv, st);
 }
 
 int nkr_b200_spmv(nkr_b200_ctx *ctx, uint64_t rows, uint64_t cols, const uint32_t *row_ptr,

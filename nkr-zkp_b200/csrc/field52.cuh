@@ -13,7 +13,7 @@
 // the offsets' bit patterns are the integers; the 25 limb products of a x b
 // are independent, columns are summed as 64-bit integers and the offsets are
 // removed once per column.  The reduction is word-serial Montgomery with
-// 52-bit words (q = t * (-p^-1) mod 2^52, also by FMA).
+// 52-bit words (q = t * (-p^-1) mod 2^52 by integer multiply; q * p by FMA).
 //
 // Representation: limbs are uint64 integers < 2^52, values canonical (< p),
 // Montgomery form with R' = 2^260.  In memory these values are stored in the
@@ -80,6 +80,7 @@ __device__ __forceinline__ void mul_wide(double a, double b, uint64_t &lo_b, uin
     lo_b = static_cast<uint64_t>(__double_as_longlong(l));
 }
 
+
 // s (five 52-bit limbs, value < 2p) minus p when s >= p
 __device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
 {
@@ -145,7 +146,6 @@ __device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *con
             bias[i + j] += kBias52;
             bias[i + j + 1] += kBias104;
         }
-    const double pinv = double(kPinv);
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
         uint64_t t[N];
@@ -153,9 +153,11 @@ __device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *con
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             t[k] = C[k][i] - bias[i]; // the column's integer value
-            uint64_t qlo, qhi;
-            mul_wide(to_double(t[k] & kMask), pinv, qlo, qhi);
-            q[k] = __longlong_as_double(static_cast<long long>(qlo)) - 0x1p52;
+            // q = t (-p^-1) mod 2^52 on the integer multiply pipe (the low 64 bits
+            // of a 52 x 52-bit product), leaving the FP64 pipe to the limb
+            // products: 160 instead of 180 FP64 instructions per product, 1.5%
+            // off a 2^20 prove
+            q[k] = to_double(((t[k] & kMask) * kPinv) & kMask);
         }
 #pragma unroll
         for (int k = 0; k < N; ++k) {

@@ -76,6 +76,8 @@ ProveSlot::~ProveSlot()
         if (e) cudaEventDestroy(e);
     for (auto e : ev_t)
         if (e) cudaEventDestroy(e);
+    for (auto e : ev_msm_end)
+        if (e) cudaEventDestroy(e);
     for (auto p : pinned_wit)
         if (p) cudaFreeHost(p);
     if (pinned_out) cudaFreeHost(pinned_out);
@@ -116,6 +118,7 @@ int slot_add(nkr_b200_key *key)
     for (auto &e : sl->ev_sorted) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : sl->ev_wit) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : sl->ev_t) NKR_CUDA(cudaEventCreate(&e));
+    for (auto &e : sl->ev_msm_end) NKR_CUDA(cudaEventCreate(&e));
     size_t bytes = 0;
     for (int g = 0; g < key->n_sorts; ++g) {
         NKR_TRY(msm_sort_alloc(sl->sort_w[g], key->bases[key->sort_stream[g]].shape));
@@ -180,6 +183,7 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
         const int g = key->sort_of[k];
         if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(sl->st[k], sl->ev_sorted[g], 0));
         NKR_TRY(msm_acc_run(key->bases[k], sl->sort_w[g], sl->acc[k], out + kOutOffset[k], sl->st[k]));
+        if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[k], sl->st[k]));
         NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
     }
     // ar and bs1 tabulated for the blinding, behind the H chain on A's stream
@@ -200,6 +204,7 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[2], s0));
     NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, sl->sort_h, h, s0));
     NKR_TRY(msm_acc_run(key->bases[kMsmH], sl->sort_h, sl->acc[kMsmH], out + kOutOffset[kMsmH], s0));
+    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[kMsmH], s0));
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[3], s0));
     for (int k : kWitnessOrder) NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_done[k], 0));
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[4], s0));
@@ -272,9 +277,9 @@ int slot_upload_witness(nkr_b200_key *key, ProveSlot *sl, const void *witness)
     return NKR_B200_OK;
 }
 
-int slot_launch(ProveSlot *sl)
+int slot_launch(ProveSlot *sl, cudaStream_t launch)
 {
-    NKR_CUDA(cudaGraphLaunch(sl->graph_exec, sl->main()));
+    NKR_CUDA(cudaGraphLaunch(sl->graph_exec, launch ? launch : sl->main()));
     g_kernel_launches.fetch_add(sl->graph_kernels, std::memory_order_relaxed);
     return NKR_B200_OK;
 }
@@ -399,6 +404,14 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     key->times.quotient_msm_ms = ms[2];
     NKR_CUDA(cudaEventElapsedTime(&key->times.total_ms, sl->ev_t[0], sl->ev_t[4]));
     key->times.witness_msms_ms = key->times.total_ms - ms[0];
+    float *ends[kNumMsm];
+    ends[kMsmA] = &key->times.msm_a_end_ms;
+    ends[kMsmB1] = &key->times.msm_b_g1_end_ms;
+    ends[kMsmB2] = &key->times.msm_b_g2_end_ms;
+    ends[kMsmL] = &key->times.msm_l_end_ms;
+    ends[kMsmH] = &key->times.msm_h_end_ms;
+    for (int k = 0; k < kNumMsm; ++k)
+        NKR_CUDA(cudaEventElapsedTime(ends[k], sl->ev_t[0], sl->ev_msm_end[k]));
     key->have_times = true;
     return NKR_B200_OK;
 }

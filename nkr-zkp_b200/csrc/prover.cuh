@@ -61,6 +61,7 @@ struct ProveSlot {
     cudaStream_t st[kNumMsm] = {};
     cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
+    cudaEvent_t ev_msm_end[kNumMsm] = {}; // timed proves: each MSM's end on its stream
     // the prove as a graph (witness already in z); kernels launched per replay
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -114,7 +115,9 @@ int slot_capture(nkr_b200_key *key, ProveSlot *slot);
 // slot's main stream; pageable input goes through the slot's pinned double buffer.
 int slot_upload_witness(nkr_b200_key *key, ProveSlot *slot, const void *witness);
 // Replays the slot's graph on its main stream.
-int slot_launch(ProveSlot *slot);
+// Replays the slot's captured prove graph into `launch` (default: the slot's main
+// stream); the graph's kernels run at that stream's priority.
+int slot_launch(ProveSlot *slot, cudaStream_t launch = nullptr);
 // Blinding buffers and the fixed-base tables of the key's alpha1, beta1, delta1
 // and delta2 (pk_const already resident); synchronises st.
 int blind_tables_build(nkr_b200_key *key, cudaStream_t st);

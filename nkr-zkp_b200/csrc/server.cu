@@ -13,7 +13,15 @@
 //     slot's streams, so requests of different keys (and several of one key)
 //     overlap on the device while earlier ones are still running,
 //   - polls the slots' completion events, normalises finished raw proofs and
-//     wakes their waiters.
+//     wakes their waiters,
+//   - ages waiting requests: one that waited longer than age_factor times its
+//     key's recent service time (an average over its completed requests) is
+//     launched into a stream of the device's highest priority instead of the
+//     slot's own, so the block scheduler no longer serves it after every
+//     smaller proof (captured graphs run at the priority of the stream they are
+//     launched into).  Without ageing, the largest circuit's requests absorb the
+//     priority given to the small ones and their tail latency exceeds that of a
+//     plain FIFO queue.
 // A request's result does not depend on what else is in flight: every slot has
 // its own buffers and the resident key data is read only.
 #include <algorithm>
@@ -39,6 +47,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     uint64_t id = 0;
     int key_id = 0;
+    bool aged = false;
     const void *witness = nullptr;
     Clock::time_point t_submit, t_start, t_done;
     bool done = false;
@@ -50,12 +59,15 @@ struct Request {
 struct SlotState {
     ProveSlot *slot = nullptr;
     cudaEvent_t ev_finish = nullptr;
+    cudaEvent_t ev_ready = nullptr;   // the witness upload, for an aged launch
+    cudaStream_t urgent = nullptr;    // highest-priority launch stream (made on first use)
     Request *req = nullptr; // in flight on this slot
 };
 
 struct KeyState {
     nkr_b200_key *key = nullptr;
     std::vector<SlotState> slots;
+    double service_ms = 0; // running average of t_done - t_start (0: none completed yet)
 };
 
 } // namespace
@@ -66,6 +78,7 @@ struct nkr_b200_server {
     nkr_b200_ctx *ctx = nullptr;
     int max_inflight = 8;
     int max_slots_per_key = 4;
+    double age_factor = 1.0; // 0: no ageing
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::vector<nkr::KeyState> keys;
@@ -76,7 +89,7 @@ struct nkr_b200_server {
     bool stop = false;
     std::thread worker;
     // statistics
-    uint64_t completed = 0, failed = 0;
+    uint64_t completed = 0, failed = 0, aged = 0;
     double busy_first_ms = -1, busy_last_ms = 0;
     nkr::Clock::time_point t0 = nkr::Clock::now();
 };
@@ -99,6 +112,20 @@ double ms_since(const Clock::time_point &a, const Clock::time_point &b)
 int key_slot_cap(const nkr_b200_server *sv, const nkr_b200_key *key)
 {
     return key->logn >= 19 ? 1 : sv->max_slots_per_key;
+}
+
+// The slot's highest-priority launch stream (created on first use) and the event
+// that orders it after the witness upload on the slot's main stream.
+int aged_stream(SlotState *st, cudaStream_t *out)
+{
+    if (!st->urgent) {
+        int least = 0, greatest = 0;
+        NKR_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        NKR_CUDA(cudaStreamCreateWithPriority(&st->urgent, cudaStreamNonBlocking, greatest));
+        NKR_CUDA(cudaEventCreateWithFlags(&st->ev_ready, cudaEventDisableTiming));
+    }
+    *out = st->urgent;
+    return NKR_B200_OK;
 }
 
 // Start request r on a free slot of its key; returns false when none can be had.
@@ -137,14 +164,24 @@ bool try_start(nkr_b200_server *sv, Request *r)
     if (!free_slot) return false;
     ProveSlot *sl = free_slot->slot;
     r->t_start = Clock::now();
+    r->aged = sv->age_factor > 0 && ks.service_ms > 0 &&
+              ms_since(r->t_submit, r->t_start) > sv->age_factor * ks.service_ms;
     int s = slot_upload_witness(ks.key, sl, r->witness);
-    if (s == NKR_B200_OK) s = slot_launch(sl);
+    cudaStream_t launch = sl->main();
+    if (s == NKR_B200_OK && r->aged) {
+        s = aged_stream(free_slot, &launch);
+        if (s == NKR_B200_OK && (cudaEventRecord(free_slot->ev_ready, sl->main()) != cudaSuccess ||
+                                 cudaStreamWaitEvent(launch, free_slot->ev_ready, 0) != cudaSuccess))
+            s = NKR_B200_ECUDA;
+    }
+    if (s == NKR_B200_OK) s = slot_launch(sl, launch);
     if (s == NKR_B200_OK &&
-        cudaMemcpyAsync(sl->pinned_out, sl->out.p, kOutBytes, cudaMemcpyDeviceToHost, sl->main()) !=
+        cudaMemcpyAsync(sl->pinned_out, sl->out.p, kOutBytes, cudaMemcpyDeviceToHost, launch) !=
             cudaSuccess)
         s = NKR_B200_ECUDA;
-    if (s == NKR_B200_OK && cudaEventRecord(free_slot->ev_finish, sl->main()) != cudaSuccess)
+    if (s == NKR_B200_OK && cudaEventRecord(free_slot->ev_finish, launch) != cudaSuccess)
         s = NKR_B200_ECUDA;
+    if (s == NKR_B200_OK && r->aged) ++sv->aged;
     if (s != NKR_B200_OK) {
         r->status = s;
         r->error = get_error();
@@ -192,6 +229,8 @@ void worker_loop(nkr_b200_server *sv)
                     normalize_raw(s.slot->pinned_out);
                     raw_from_bytes(s.slot->pinned_out, &r->raw);
                     ++sv->completed;
+                    const double svc = ms_since(r->t_start, r->t_done);
+                    ks.service_ms = ks.service_ms > 0 ? 0.75 * ks.service_ms + 0.25 * svc : svc;
                 }
                 r->done = true;
                 const double t_ms = ms_since(sv->t0, r->t_done);
@@ -285,6 +324,24 @@ int nkr_b200_server_wait(nkr_b200_server *sv, uint64_t request_id, nkr_b200_raw_
     return status;
 }
 
+int nkr_b200_server_set_ageing(nkr_b200_server *sv, double age_factor)
+{
+    NKR_REQUIRE(sv && age_factor >= 0, "bad argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->age_factor = age_factor;
+    return NKR_B200_OK;
+}
+
+int nkr_b200_server_stats(nkr_b200_server *sv, uint64_t *completed, uint64_t *failed, uint64_t *aged)
+{
+    NKR_REQUIRE(sv, "null argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    if (completed) *completed = sv->completed;
+    if (failed) *failed = sv->failed;
+    if (aged) *aged = sv->aged;
+    return NKR_B200_OK;
+}
+
 int nkr_b200_server_slots(nkr_b200_server *sv, int key_id, int *slots)
 {
     NKR_REQUIRE(sv && slots, "null argument");
@@ -305,8 +362,11 @@ void nkr_b200_server_destroy(nkr_b200_server *sv)
     if (sv->worker.joinable()) sv->worker.join();
     cudaSetDevice(sv->ctx->device);
     for (auto &ks : sv->keys)
-        for (auto &s : ks.slots)
+        for (auto &s : ks.slots) {
             if (s.ev_finish) cudaEventDestroy(s.ev_finish);
+            if (s.ev_ready) cudaEventDestroy(s.ev_ready);
+            if (s.urgent) cudaStreamDestroy(s.urgent);
+        }
     delete sv;
 }
 

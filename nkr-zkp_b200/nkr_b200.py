@@ -63,7 +63,9 @@ class VerificationKeyC(ctypes.Structure):
 
 class StageTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in
-                ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms")]
+                ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms",
+                 "msm_a_end_ms", "msm_b_g1_end_ms", "msm_b_g2_end_ms", "msm_l_end_ms",
+                 "msm_h_end_ms")]
 
 
 class MsmStats(ctypes.Structure):
@@ -115,6 +117,9 @@ _SIGS = {
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
     "nkr_b200_server_slots": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "nkr_b200_server_set_ageing": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "nkr_b200_server_stats": (ctypes.c_int, [_VP, ctypes.POINTER(_U64), ctypes.POINTER(_U64),
+                                             ctypes.POINTER(_U64)]),
     "nkr_b200_server_destroy": (None, [_VP]),
     "nkr_b200_set_autotune": (ctypes.c_int, [_VP, ctypes.c_int]),
     "nkr_b200_tune_msm": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(ctypes.c_int),
@@ -660,6 +665,15 @@ class Server:
         n = ctypes.c_int()
         _check(_lib.nkr_b200_server_slots(self.h, key_id, ctypes.byref(n)), "server_slots")
         return n.value
+
+    def set_ageing(self, age_factor):
+        _check(_lib.nkr_b200_server_set_ageing(self.h, float(age_factor)), "server_set_ageing")
+
+    def stats(self):
+        c, f, a = _U64(), _U64(), _U64()
+        _check(_lib.nkr_b200_server_stats(self.h, ctypes.byref(c), ctypes.byref(f), ctypes.byref(a)),
+               "server_stats")
+        return {"completed": c.value, "failed": f.value, "aged": a.value}
 
     def close(self):
         if self.h:
