@@ -976,6 +976,8 @@ def run_kernels(args):
         return {"op": f"msm.g{group}.{mix}", "n": f"2^{logn}", "ms": round(ms, 4),
                 "window_bits": st["window_bits"], "windows": st["windows"], "entries": st["entries"],
                 "acc_ms": round(acc_ms, 4), "G_fq_mul_per_s_acc": round(muls / acc_ms / 1e6, 2),
+                "phases_ms": {k: round(st[k], 4) for k in ("sort_ms", "acc_ms", "fixup_ms",
+                                                            "reduce_first_ms", "reduce_levels_ms")},
                 "frac_fq_mul_peak_acc": round(muls / (acc_ms * 1e-3) / fq_peak, 3),
                 "G_fq_mul_per_s_whole": round(muls / ms / 1e6, 2),
                 "GB_per_s_algorithmic": round(byts / ms / 1e6, 1),
@@ -1118,7 +1120,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.8)
     ap.add_argument("--serve-sat-load", type=float, default=1.5)
-    ap.add_argument("--serve-age", type=float, default=1.0)
+    ap.add_argument("--serve-age", type=float, default=0.5)
     ap.add_argument("--serve-inflight", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":

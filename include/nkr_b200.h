@@ -205,7 +205,7 @@ int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses
  * captured prove graph, so requests of different circuits overlap on the GPU.
  * Slot streams take a priority by circuit size, so the GPU's block scheduler
  * serves the smaller proofs in flight first (low median latency).  Requests
- * age: one that waited longer than age_factor (default 1) times its key's
+ * age: one that waited longer than age_factor (default 0.5) times its key's
  * recent service time is launched at the device's highest stream priority, so
  * the largest circuit's requests do not absorb all of the small ones' priority.
  * The witness memory of a request must stay valid until its wait returns.
@@ -332,11 +332,14 @@ void nkr_b200_msm_bases_free(nkr_b200_msm_bases *b);
 /* Statistics of the last nkr_b200_msm_bases_run: device time of the whole MSM
  * and of the bucket-accumulation kernel (CUDA events on its stream), the number
  * of (point, nonzero digit) entries it accumulated, accumulation tasks, window
- * shape and bucket count. */
+ * shape and bucket count; then the other phases' device times: the digit sort,
+ * the fix-up levels of buckets spread over many segments, the first bucket
+ * reduction level, and the remaining reduction levels with the final combination. */
 typedef struct {
     float total_ms, acc_ms;
     uint64_t entries, tasks;
     uint32_t window_bits, windows, buckets;
+    float sort_ms, fixup_ms, reduce_first_ms, reduce_levels_ms;
 } nkr_b200_msm_stats;
 int nkr_b200_msm_bases_stats(const nkr_b200_msm_bases *b, nkr_b200_msm_stats *out);
 

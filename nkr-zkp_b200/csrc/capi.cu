@@ -434,8 +434,7 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     NKR_TRY(tuned_window_bits(ctx, idx.size(), &c));
     NKR_TRY(msm_bases_build_support(h->bases, group, bases, n, std::move(idx), true, c, ctx->stream));
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
-    NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[0]));
-    NKR_CUDA(cudaEventCreate(&h->scratch.acc.ev_acc[1]));
+    for (auto &e : h->scratch.acc.ev_acc) NKR_CUDA(cudaEventCreate(&e));
     h->scratch.acc.timing = true;
     NKR_TRY(h->scalars.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
     *out = h.release();
@@ -475,15 +474,18 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
     float total = 0.f;
     cudaEventElapsedTime(&total, e0, e1);
     if (device_ms) *device_ms = total;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (s == NKR_B200_OK) {
         if (b->bases.group == 1)
             host::normalize_g1(out);
         else
             host::normalize_g2(out);
         b->last.total_ms = total;
-        NKR_CUDA(cudaEventElapsedTime(&b->last.acc_ms, b->scratch.acc.ev_acc[0], b->scratch.acc.ev_acc[1]));
+        const cudaEvent_t *ev = b->scratch.acc.ev_acc;
+        NKR_CUDA(cudaEventElapsedTime(&b->last.sort_ms, e0, ev[0]));
+        NKR_CUDA(cudaEventElapsedTime(&b->last.acc_ms, ev[0], ev[1]));
+        NKR_CUDA(cudaEventElapsedTime(&b->last.fixup_ms, ev[1], ev[2]));
+        NKR_CUDA(cudaEventElapsedTime(&b->last.reduce_first_ms, ev[2], ev[3]));
+        NKR_CUDA(cudaEventElapsedTime(&b->last.reduce_levels_ms, ev[3], ev[4]));
         uint32_t entries = 0, tasks = 0;
         const uint32_t nb = b->bases.shape.nb;
         NKR_CUDA(cudaMemcpy(&entries, b->scratch.sort.offsets.as<uint32_t>() + nb, 4, cudaMemcpyDeviceToHost));
@@ -494,6 +496,8 @@ int nkr_b200_msm_bases_run(nkr_b200_msm_bases *b, const void *scalars, uint64_t 
         b->last.windows = uint32_t(b->bases.shape.W);
         b->last.buckets = nb;
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return s;
 }
 

@@ -152,60 +152,6 @@ __device__ __forceinline__ Affine<CF<F>> lda(const Affine<F> &s)
     return {msm_in(s.x), msm_in(s.y)};
 }
 
-// The bucket-reduction levels are latency bound (a few long chains of dependent
-// additions), so G2 may reduce in the FP64-limb Fq2, whose products have a much
-// shorter dependency chain than the 32-bit CIOS products the G2 accumulation
-// runs; items convert at load and store (R = 2^256 storage, R' = 2^260 compute).
-template <class F>
-struct RedArith {
-    using type = CF<F>;
-};
-#ifdef NKR_G2_REDUCE_FP64
-template <>
-struct RedArith<Fq2> {
-    using type = Fq2x52;
-};
-#endif
-template <class F>
-using RF = typename RedArith<F>::type;
-
-__device__ __forceinline__ Fq2x52 red_in(const Fq2 &x)
-{
-    return {r256_to_r260(to52(x.c0)), r256_to_r260(to52(x.c1))};
-}
-__device__ __forceinline__ Fq2 red_out(const Fq2x52 &x)
-{
-    return {from52(r260_to_r256(x.c0)), from52(r260_to_r256(x.c1))};
-}
-
-template <class F>
-__device__ __forceinline__ Xyzz<RF<F>> ldr(const Xyzz<F> &s)
-{
-    if constexpr (std::is_same<RF<F>, CF<F>>::value)
-        return ldx(s);
-    else
-        return {red_in(s.x), red_in(s.y), red_in(s.zz), red_in(s.zzz)};
-}
-
-template <class F>
-__device__ __forceinline__ Xyzz<F> str(const Xyzz<RF<F>> &c)
-{
-    if constexpr (std::is_same<RF<F>, CF<F>>::value)
-        return stx(c);
-    else
-        return {red_out(c.x), red_out(c.y), red_out(c.zz), red_out(c.zzz)};
-}
-
-// a reduction-domain value in the library's storage domain (R = 2^256)
-template <class F>
-__device__ __forceinline__ F red_leave(const RF<F> &x)
-{
-    if constexpr (std::is_same<RF<F>, Fq2x52>::value)
-        return red_out(x);
-    else
-        return msm_out(msm_leave(x));
-}
-
 // first index in a[0, n) with a[idx] > x (a nondecreasing)
 __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t *a, uint32_t n, uint32_t x)
 {
@@ -324,7 +270,8 @@ __device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets
 // 3-blocks-per-SM register budget: measured against the compiler's own choice
 // (184 registers, 2 blocks) and a 4-block budget (128 registers, more spills),
 // it is the fastest from 2^16 to 2^20 points, uniform and sparse.  G2 keeps the
-// compiler's choice.
+// compiler's choice (232 registers, 2 blocks per SM; a 3-block budget spills 284 B
+// per thread and is no faster).
 template <class F>
 __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
                                                  const uint32_t *__restrict__ entries,
@@ -414,7 +361,7 @@ int first_level_log2(uint32_t m, int log2_bs)
 // (one piece) or by the fix-up levels (more than kSmallPieces pieces), or else
 // its few pieces are added straight from the partial slots.
 template <class F>
-__device__ __forceinline__ Xyzz<RF<F>> add_bucket_sum(Xyzz<RF<F>> run,
+__device__ __forceinline__ Xyzz<CF<F>> add_bucket_sum(Xyzz<CF<F>> run,
                                                       const uint32_t *__restrict__ offsets,
                                                       const Xyzz<F> *__restrict__ partials,
                                                       const Xyzz<F> *__restrict__ buckets, uint32_t b,
@@ -423,8 +370,8 @@ __device__ __forceinline__ Xyzz<RF<F>> add_bucket_sum(Xyzz<RF<F>> run,
     const uint32_t lo = offsets[b], hi = offsets[b + 1];
     if (hi == lo) return run;
     const Pieces pc{lo / k1, (hi - 1) / k1 - lo / k1 + 1};
-    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldr(buckets[b]));
-    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldr(partials[pc.slot(lo, k1, k)]));
+    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldx(buckets[b]));
+    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldx(partials[pc.slot(lo, k1, k)]));
     return run;
 }
 
@@ -443,13 +390,13 @@ __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict
     const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t * L >= items) return;
     const uint64_t base = t * L;
-    Xyzz<RF<F>> run = Xyzz<RF<F>>::inf(), tri = Xyzz<RF<F>>::inf();
+    Xyzz<CF<F>> run = Xyzz<CF<F>>::inf(), tri = Xyzz<CF<F>>::inf();
     for (int i = int(L) - 1; i >= 0; --i) {
         run = add_bucket_sum(run, offsets, partials, buckets, uint32_t(base + i), k1);
         if (i > 0) tri = xyzz_add(tri, run);
     }
-    a_out[t] = str<F>(tri);
-    r_out[t] = str<F>(run);
+    a_out[t] = stx(tri);
+    r_out[t] = stx(run);
 }
 
 // One level of the weighted sum: items carry (A_c, R_c) with
@@ -467,7 +414,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
                                                       Xyzz<F> *__restrict__ a_out,
                                                       Xyzz<F> *__restrict__ r_out)
 {
-    using C = RF<F>;
+    using C = CF<F>;
     extern __shared__ uint8_t smem_raw[];
     Xyzz<C> *buf0 = reinterpret_cast<Xyzz<C> *>(smem_raw);
     Xyzz<C> *buf1 = buf0 + BS;
@@ -478,7 +425,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     const uint64_t idx = uint64_t(blk) * BS + i;
     const bool live = idx < m;
     const uint64_t g = uint64_t(set) * m + idx;
-    Xyzz<C> v = live ? ldr(r_in[g]) : Xyzz<C>::inf();
+    Xyzz<C> v = live ? ldx(r_in[g]) : Xyzz<C>::inf();
     buf0[i] = v;
     __syncthreads();
     Xyzz<C> *cur = buf0, *nxt = buf1;
@@ -494,7 +441,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     const Xyzz<C> total = cur[0];
     __syncthreads();
     buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
-    buf1[i] = (a_in && live) ? ldr(a_in[g]) : Xyzz<C>::inf();
+    buf1[i] = (a_in && live) ? ldx(a_in[g]) : Xyzz<C>::inf();
     __syncthreads();
     for (int s = BS / 2; s > 0; s >>= 1) {
         if (i < s) {
@@ -507,8 +454,8 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
         Xyzz<C> w = buf0[0];
         for (int d = 0; d < log2_unit; ++d) w = xyzz_dbl(w);
         const uint32_t o = set * blocks_per_set + blk;
-        a_out[o] = str<F>(xyzz_add(w, buf1[0]));
-        r_out[o] = str<F>(total);
+        a_out[o] = stx(xyzz_add(w, buf1[0]));
+        r_out[o] = stx(total);
     }
 }
 
@@ -516,9 +463,9 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
 // X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point; the
 // coordinates leave the R' domain here (back to the library's R = 2^256).
 template <class F>
-__device__ __forceinline__ void store_jacobian(const Xyzz<RF<F>> &p, F *out)
+__device__ __forceinline__ void store_jacobian(const Xyzz<CF<F>> &p, F *out)
 {
-    using C = RF<F>;
+    using C = CF<F>;
     if (p.is_inf()) {
         out[0] = F::zero();
         out[1] = F::one();
@@ -527,21 +474,21 @@ __device__ __forceinline__ void store_jacobian(const Xyzz<RF<F>> &p, F *out)
     }
     const C zzz2 = sqr(p.zzz);
     const C zz2 = sqr(p.zz);
-    out[0] = red_leave<F>(p.x * (p.zz * zzz2));
-    out[1] = red_leave<F>(p.y * (zz2 * p.zz * zzz2));
-    out[2] = red_leave<F>(p.zz * p.zzz);
+    out[0] = msm_out(msm_leave(p.x * (p.zz * zzz2)));
+    out[1] = msm_out(msm_leave(p.y * (zz2 * p.zz * zzz2)));
+    out[2] = msm_out(msm_leave(p.zz * p.zzz));
 }
 
 template <class F>
 __global__ void k_finalize(const Xyzz<F> *a, const Xyzz<F> *r, int sets, int c, F *out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    using C = RF<F>;
+    using C = CF<F>;
     Xyzz<C> acc = Xyzz<C>::inf();
     for (int k = sets - 1; k >= 0; --k) {
         if (k != sets - 1)
             for (int d = 0; d < c; ++d) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, a ? xyzz_add(ldr(a[k]), ldr(r[k])) : ldr(r[k]));
+        acc = xyzz_add(acc, a ? xyzz_add(ldx(a[k]), ldx(r[k])) : ldx(r[k]));
     }
     store_jacobian<F>(acc, out);
 }
@@ -732,6 +679,7 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
                                                             uint32_t(k2));
         NKR_CHECK_LAUNCH();
     }
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[2], st));
     // bucket reduction levels
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     uint32_t m = sh.B;
@@ -739,7 +687,7 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
     constexpr int BS = sizeof(F) == sizeof(Fq) ? 256 : 128; // G1: 256 buckets per block, G2: 128
     constexpr int kLog2BS = BS == 256 ? 8 : 7;
-    const size_t smem = 2 * BS * sizeof(Xyzz<RF<F>>);
+    const size_t smem = 2 * BS * sizeof(Xyzz<CF<F>>);
     NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
     // first level: bucket sums (few-piece buckets finished here), L buckets per thread
@@ -750,6 +698,7 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
         offsets, a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), items, L, uint32_t(sh.k1), bufs_a[0],
         bufs_r[0]);
     NKR_CHECK_LAUNCH();
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[3], st));
     const Xyzz<F> *a_in = bufs_a[0];
     const Xyzz<F> *r_in = bufs_r[0];
     int flip = 1;
@@ -768,6 +717,7 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     }
     k_finalize<F><<<1, 32, 0, st>>>(a_in, r_in, int(sets), sh.c, static_cast<F *>(out_dev));
     NKR_CHECK_LAUNCH();
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[4], st));
     return NKR_B200_OK;
 }
 

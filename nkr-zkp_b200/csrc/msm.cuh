@@ -80,8 +80,11 @@ struct MsmSort {
 // Accumulation state of one MSM (partials, buckets, reduction levels, result).
 struct MsmAcc {
     DevBuf partials, buckets, lead_off, red_a, red_r, red_a2, red_r2, scan_tmp, result;
-    bool timing = false; // record events around the level-1 accumulation kernel
-    cudaEvent_t ev_acc[2] = {nullptr, nullptr};
+    // record events at the phase boundaries: before and after the level-1
+    // accumulation kernel, after the fix-up levels, after the first reduction
+    // level, after the last reduction level and the final combination
+    bool timing = false;
+    cudaEvent_t ev_acc[5] = {};
     size_t device_bytes() const
     {
         return partials.bytes + buckets.bytes + lead_off.bytes + red_a.bytes + red_r.bytes +

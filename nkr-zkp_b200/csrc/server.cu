@@ -78,7 +78,7 @@ struct nkr_b200_server {
     nkr_b200_ctx *ctx = nullptr;
     int max_inflight = 8;
     int max_slots_per_key = 4;
-    double age_factor = 1.0; // 0: no ageing
+    double age_factor = 0.5; // 0: no ageing
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::vector<nkr::KeyState> keys;

@@ -71,7 +71,8 @@ class StageTimes(ctypes.Structure):
 class MsmStats(ctypes.Structure):
     _fields_ = [("total_ms", ctypes.c_float), ("acc_ms", ctypes.c_float), ("entries", _U64),
                 ("tasks", _U64), ("window_bits", ctypes.c_uint32), ("windows", ctypes.c_uint32),
-                ("buckets", ctypes.c_uint32)]
+                ("buckets", ctypes.c_uint32), ("sort_ms", ctypes.c_float), ("fixup_ms", ctypes.c_float),
+                ("reduce_first_ms", ctypes.c_float), ("reduce_levels_ms", ctypes.c_float)]
 
 
 _SIGS = {

@@ -113,3 +113,26 @@ def test_large_key_proves_one_request_at_a_time(ctx):
     sv.close()
     for be in bes:
         be.free()
+
+
+def test_aged_requests_launch_at_top_priority_and_stay_exact(ctx, keyset):
+    """With an ageing factor near zero every request that starts after its key's
+    first completion is aged (launched into the slot's highest-priority stream,
+    ordered after its witness upload); results still equal the plain proves and
+    the server counts the aged launches."""
+    backends, wits, single = keyset
+    sv = nk.Server(ctx, max_inflight=6, max_slots_per_key=2)
+    sv.set_ageing(1e-9)
+    ids = [sv.add_key(be) for be in backends]
+    for rep in range(3):
+        rids = [(j, i, sv.submit(ids[j], wits[j][i])) for j in range(len(SPECS))
+                for i in range(len(wits[j]))]
+        for j, i, r in rids:
+            assert bytes(sv.wait(r)[0]) == single[j][i], f"rep {rep} key {j} witness {i}"
+    st = sv.stats()
+    total = sum(len(w) for w in wits) * 3
+    assert st["completed"] == total and st["failed"] == 0
+    assert st["aged"] >= total - 2 * len(SPECS) * 2   # all but the first wave of each key
+    with pytest.raises(nk.B200Error):
+        sv.set_ageing(-1.0)
+    sv.close()
