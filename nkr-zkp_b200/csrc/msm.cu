@@ -404,8 +404,9 @@ __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict
 // buckets, U = 1).  A block takes BS consecutive
 // items c (padding with infinity), forms the suffix sums Suf_c = sum_{c' >= c} R_c'
 // with a Hillis-Steele scan in shared memory (log2 BS dependent additions),
-// then sum_c c R_c = sum_{c >= 1} Suf_c and sum_c A_c by tree sums, so a level
-// costs about 2 log2(BS) dependent additions instead of 2 BS.
+// then sum_c c R_c = sum_{c >= 1} Suf_c and sum_c A_c by two tree sums on
+// disjoint threads, so a level costs about 2 log2(BS) dependent additions
+// instead of 2 BS.
 // Output per block: A' = sum A_c + U sum_c c R_c, R' = sum R_c.
 template <class F, int BS>
 __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__ a_in,
@@ -443,10 +444,14 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
     buf1[i] = (a_in && live) ? ldx(a_in[g]) : Xyzz<C>::inf();
     __syncthreads();
+    // the two tree sums run side by side on disjoint threads (first s: weighted
+    // suffix sums, next s: A items), one addition per thread and step
     for (int s = BS / 2; s > 0; s >>= 1) {
         if (i < s) {
             buf0[i] = xyzz_add(buf0[i], buf0[i + s]);
-            buf1[i] = xyzz_add(buf1[i], buf1[i + s]);
+        } else if (i < 2 * s) {
+            const int j = i - s;
+            buf1[j] = xyzz_add(buf1[j], buf1[j + s]);
         }
         __syncthreads();
     }
