@@ -109,7 +109,15 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
 // values in the 8 x 32-bit layout of Fq, converted at entry (bases) and exit
 // (result).  G2 arithmetic stays on the integer pipe (Fq2, R = 2^256): measured,
 // its FP64 form (Fq2 products as three interleaved 52-bit products) needs all 255
-// registers and ran 34% slower at 2^18 points.
+// registers and ran 34% slower at 2^18 points.  The same holds for the G2
+// reduction levels alone, although they are latency bound (a 32-bit product is
+// one long carry chain): in the FP64 form they spill 600 B per thread and took
+// 1.81 instead of 1.53 ms at 2^18; with the three Karatsuba products of an Fq2
+// product interleaved in one 32-bit call they took 1.66 ms, no faster.  Moving one
+// Karatsuba product of every Fq2 product to the FP64 pipe ((16 x) y 2^-260 =
+// x y 2^-256) relieves the integer multiply pipe but costs four doublings, limb
+// conversions and spills at 255 registers: the G2 accumulation took 4.01 instead
+// of 3.48 ms at 2^18.
 // --------------------------------------------------------------------------
 
 template <class F>
