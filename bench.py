@@ -598,9 +598,11 @@ def run_batch(args):
     first = [bytes(be.prove(None, witness_ptr=p)) for be, p in zip(bes, ptrs)]
     for _ in range(args.warmup):
         out = nk.prove_batch(bes, witness_ptrs=ptrs)
+        out_l = nk.prove_batch(bes, witness_ptrs=ptrs, lists=True)
     assert [bytes(o) for o in out] == first, "batched proofs differ from the plain proves"
+    assert [bytes(o) for o in out_l] == first, "cross-proof batched proofs differ from the plain proves"
     clocks.start()
-    seq, bat = [], []
+    seq, bat, lst = [], [], []
     launches0 = nk.launch_count()
     for _ in range(args.steps):
         t = time.perf_counter()
@@ -611,11 +613,16 @@ def run_batch(args):
         out = nk.prove_batch(bes, witness_ptrs=ptrs)
         bat.append(time.perf_counter() - t)
         assert [bytes(o) for o in out] == first
+        t = time.perf_counter()
+        out = nk.prove_batch(bes, witness_ptrs=ptrs, lists=True)
+        lst.append(time.perf_counter() - t)
+        assert [bytes(o) for o in out] == first
     launches = (nk.launch_count() - launches0) // max(args.steps, 1)
     clk = clocks.stop()
     n = len(mix)
     seq_pps = n / statistics.median(seq)
     bat_pps = n / statistics.median(bat)
+    lst_pps = n / statistics.median(lst)
     hist = {}
     for r in rows:
         hist[f"2^{r.bit_length() - 1}"] = hist.get(f"2^{r.bit_length() - 1}", 0) + 1
@@ -630,6 +637,11 @@ def run_batch(args):
         "plain_sequential": {"value": round(seq_pps, 2), "unit": "proofs/s",
                              "path": "nkr_b200_prove one proof at a time (upload, prove, download)"},
         "speedup_vs_plain": round(bat_pps / seq_pps, 3),
+        "cross_proof_lists": {"value": round(lst_pps, 2), "unit": "proofs/s",
+                              "speedup_vs_plain": round(lst_pps / seq_pps, 3),
+                              "path": "nkr_b200_prove_batch_lists: per wave one launch per NTT "
+                                      "pass, quotient step and level-1 accumulation over all "
+                                      "proofs (device work lists)"},
         "e2e": {"value": round(bat_pps, 2), "unit": "proofs/s",
                 "h2d_bytes_per_step": sum(t.numel() * 8 for t in pins),
                 "d2h_bytes_per_step": 576 * n},

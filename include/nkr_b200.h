@@ -195,6 +195,17 @@ int nkr_b200_key_stage_times(const nkr_b200_key *key, nkr_b200_stage_times *out)
  * graphs.  witnesses[i] has keys[i]'s cols elements. */
 int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
                          nkr_b200_raw_proof *out);
+/* The same batch with cross-proof launches: the proofs run in waves of at most
+ * one proof per prove slot, and within a wave every NTT pass of every proof's
+ * quotient chain (transforms of any sizes), the pointwise quotient step of all
+ * proofs, and the level-1 bucket accumulation of all G1 witness MSMs, of all G2
+ * MSMs and of all H MSMs each run as ONE launch over a device work list; the
+ * per-proof steps (SpMV, digit sorts, fix-up and reduction levels) run on the
+ * proofs' own slot streams beside them.  Results equal nkr_b200_prove_batch's
+ * bit for bit.  No counterpart in the reference, which batches by running
+ * separate processes (scripts/bench/runner.py:260-354). */
+int nkr_b200_prove_batch_lists(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                               nkr_b200_raw_proof *out);
 
 /* ---- request server (continuous batching over resident keys) -------------
  * No counterpart in the reference, which proves one request per process

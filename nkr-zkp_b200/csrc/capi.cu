@@ -104,6 +104,7 @@ int key_blind(nkr_b200_key *, const nkr_b200_raw_proof *, const void *, const vo
               nkr_b200_proof *);
 int key_intermediates(nkr_b200_key *, void *, void *, void *, void *);
 int key_prove_batch(nkr_b200_key *const *, const void *const *, int, nkr_b200_raw_proof *);
+int key_prove_batch_lists(nkr_b200_key *const *, const void *const *, int, nkr_b200_raw_proof *);
 
 int ctx_check(nkr_b200_ctx *ctx)
 {
@@ -213,6 +214,12 @@ int nkr_b200_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses
                          nkr_b200_raw_proof *out)
 {
     return key_prove_batch(keys, witnesses, count, out);
+}
+
+int nkr_b200_prove_batch_lists(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                               nkr_b200_raw_proof *out)
+{
+    return key_prove_batch_lists(keys, witnesses, count, out);
 }
 
 int nkr_b200_ntt(nkr_b200_ctx *ctx, int op, void *data, uint64_t n)

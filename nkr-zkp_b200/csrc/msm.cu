@@ -229,10 +229,9 @@ __device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets
                                             const uint32_t *__restrict__ entries,
                                             const Affine<F> *__restrict__ pts, uint32_t nb,
                                             uint32_t k1, Xyzz<F> *__restrict__ partials,
-                                            Xyzz<F> *__restrict__ buckets)
+                                            Xyzz<F> *__restrict__ buckets, uint32_t t)
 {
     const uint32_t total = offsets[nb];
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t beg64 = uint64_t(t) * k1;
     if (beg64 >= total) return;
     const uint32_t beg = uint32_t(beg64);
@@ -287,7 +286,7 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
                                                  uint32_t k1, Xyzz<F> *__restrict__ partials,
                                                  Xyzz<F> *__restrict__ buckets)
 {
-    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets);
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <class F>
@@ -298,7 +297,46 @@ __global__ void __launch_bounds__(128, 3) k_acc_l1_g1(const uint32_t *__restrict
                                                        Xyzz<F> *__restrict__ partials,
                                                        Xyzz<F> *__restrict__ buckets)
 {
-    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets);
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Level 1 of several MSMs of one group in one launch (a batch's MSMs, any sizes):
+// item i owns blocks [first_block, next item's first_block) of the grid.
+template <class F>
+struct AccItem {
+    const uint32_t *offsets, *entries;
+    const Affine<F> *pts;
+    Xyzz<F> *partials, *buckets;
+    uint32_t nb, k1, first_block;
+};
+static_assert(sizeof(AccItem<Fq>) <= kMsmAccItemBytes, "work-list item size");
+
+template <class F>
+__device__ __forceinline__ void acc_l1_list_body(const AccItem<F> *items, int n_items)
+{
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= blockIdx.x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const AccItem<F> it = items[lo];
+    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
+                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x);
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_acc_l1_list(const AccItem<F> *items, int n_items)
+{
+    acc_l1_list_body(items, n_items);
+}
+
+template <class F>
+__global__ void __launch_bounds__(128, 3) k_acc_l1_g1_list(const AccItem<F> *items, int n_items)
+{
+    acc_l1_list_body(items, n_items);
 }
 
 // One group of k2 pieces (spaced `stride` pieces apart) of one bucket; the
@@ -661,7 +699,7 @@ int build_windows_t(MsmBases &b, cudaStream_t st)
 }
 
 template <class F>
-int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+int acc_level1_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, cudaStream_t st)
 {
     const MsmShape &sh = bs.shape;
     // no bucket clearing: a bucket is read only after the kernel that wrote it
@@ -678,6 +716,47 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
             a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[1], st));
+    return NKR_B200_OK;
+}
+
+// Level 1 of n MSMs of one group in one launch; items_dev is device scratch of n
+// work-list items.
+template <class F>
+int acc_level1_list_t(const MsmAccJob *jobs, int n, void *items_host, void *items_dev, cudaStream_t st)
+{
+    if (n <= 0) return NKR_B200_OK;
+    AccItem<F> *items = static_cast<AccItem<F> *>(items_host);
+    uint64_t blocks = 0;
+    for (int i = 0; i < n; ++i) {
+        const MsmShape &sh = jobs[i].bases->shape;
+        AccItem<F> &it = items[i];
+        it.offsets = jobs[i].sort->offsets.as<uint32_t>();
+        it.entries = jobs[i].sort->entries.as<uint32_t>();
+        it.pts = jobs[i].bases->pts.as<Affine<F>>();
+        it.partials = jobs[i].acc->partials.as<Xyzz<F>>();
+        it.buckets = jobs[i].acc->buckets.as<Xyzz<F>>();
+        it.nb = sh.nb;
+        it.k1 = uint32_t(sh.k1);
+        it.first_block = uint32_t(blocks);
+        blocks += blocks_for(sh.segments_max(), 128);
+        NKR_REQUIRE(blocks < (uint64_t(1) << 31), "batched accumulation too large");
+    }
+    AccItem<F> *d = static_cast<AccItem<F> *>(items_dev);
+    NKR_CUDA(cudaMemcpyAsync(d, items, n * sizeof(AccItem<F>), cudaMemcpyHostToDevice, st));
+    if constexpr (std::is_same<F, Fq>::value)
+        k_acc_l1_g1_list<F><<<unsigned(blocks), 128, 0, st>>>(d, n);
+    else
+        k_acc_l1_list<F><<<unsigned(blocks), 128, 0, st>>>(d, n);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+template <class F>
+int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    const MsmShape &sh = bs.shape;
+    const uint64_t segs = sh.segments_max();
+    const uint32_t *offsets = s.offsets.as<uint32_t>();
     // fix-up levels: inputs spaced `stride` pieces apart, groups of k2; one
     // bucket has at most segs + 1 pieces, all buckets at most 2 segs
     const uint64_t k2 = uint64_t(sh.k2);
@@ -732,6 +811,13 @@ int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cu
     NKR_CHECK_LAUNCH();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[4], st));
     return NKR_B200_OK;
+}
+
+template <class F>
+int acc_run_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    NKR_TRY(acc_level1_t<F>(bs, s, a, st));
+    return acc_tail_t<F>(bs, s, a, out_dev, st);
 }
 
 template <class F>
@@ -939,6 +1025,21 @@ int msm_sort_run(const MsmShape &sh, MsmSort &s, const void *scalars_dev, cudaSt
 int msm_acc_run(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
     return b.group == 1 ? acc_run_t<Fq>(b, s, a, out_dev, st) : acc_run_t<Fq2>(b, s, a, out_dev, st);
+}
+
+int msm_acc_level1_list(int group, const MsmAccJob *jobs, int n, void *items_host, void *items_dev,
+                        cudaStream_t st)
+{
+    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
+    for (int i = 0; i < n; ++i)
+        NKR_REQUIRE(jobs[i].bases->group == group, "batched accumulation mixes G1 and G2");
+    return group == 1 ? acc_level1_list_t<Fq>(jobs, n, items_host, items_dev, st)
+                      : acc_level1_list_t<Fq2>(jobs, n, items_host, items_dev, st);
+}
+
+int msm_acc_tail(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    return b.group == 1 ? acc_tail_t<Fq>(b, s, a, out_dev, st) : acc_tail_t<Fq2>(b, s, a, out_dev, st);
 }
 
 int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out_dev,

@@ -145,4 +145,19 @@ int msm_acc_run(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, c
 int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out_dev,
             cudaStream_t st);
 
+// msm_acc_run in two parts, so that the level-1 accumulation of several MSMs of
+// one group (a batch of proofs) can run as one launch over a work list: the
+// level-1 kernel, then the fix-up levels, bucket reduction and final combination.
+struct MsmAccJob {
+    const MsmBases *bases;
+    const MsmSort *sort;
+    MsmAcc *acc;
+};
+constexpr size_t kMsmAccItemBytes = 64; // scratch per job of msm_acc_level1_list
+// items_host (pinned) and items_dev: n kMsmAccItemBytes items each; the host
+// items are read by the stream's copy
+int msm_acc_level1_list(int group, const MsmAccJob *jobs, int n, void *items_host, void *items_dev,
+                        cudaStream_t st);
+int msm_acc_tail(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st);
+
 } // namespace nkr

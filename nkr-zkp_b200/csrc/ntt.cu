@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 #include "ntt.cuh"
 
 namespace nkr {
@@ -102,15 +103,15 @@ __global__ void k_bitrev_scaled(const Fr *src, const Fr *c, Fr *dst, int logn)
     dst[j] = *c * src[brev_n(uint32_t(j), logn)];
 }
 
+// One tile of a pass: the group gid of 2^t elements spaced 2^s_lo apart, staged
+// through shared memory sm for t radix-2 stages.
 template <bool DIF>
-__global__ void __launch_bounds__(512) k_ntt_pass(Fr *data, int s_lo, int t, const Fr *tw,
-                                                   const Fr *pre, const Fr *post,
-                                                   const Fr *post_const)
+__device__ __forceinline__ void ntt_pass_tile(Fr *sm, Fr *data, int s_lo, int t, const Fr *tw,
+                                              const Fr *pre, const Fr *post, const Fr *post_const,
+                                              uint64_t gid)
 {
-    extern __shared__ Fr sm[];
     const int G = 1 << t;
     const int half = G >> 1;
-    const uint64_t gid = blockIdx.x;
     const uint64_t low = gid & ((uint64_t(1) << s_lo) - 1);
     const uint64_t high = gid >> s_lo;
     const uint64_t base = low | (high << (s_lo + t));
@@ -153,6 +154,54 @@ __global__ void __launch_bounds__(512) k_ntt_pass(Fr *data, int s_lo, int t, con
             x = x * *post_const;
         data[j] = x;
     }
+}
+
+template <bool DIF>
+__global__ void __launch_bounds__(512) k_ntt_pass(Fr *data, int s_lo, int t, const Fr *tw,
+                                                   const Fr *pre, const Fr *post,
+                                                   const Fr *post_const)
+{
+    extern __shared__ Fr sm[];
+    ntt_pass_tile<DIF>(sm, data, s_lo, t, tw, pre, post, post_const, blockIdx.x);
+}
+
+// One pass of many transforms (of any sizes) in one launch: item i owns blocks
+// [first_block, first_block + n >> t) of the grid.  Items are few (a batch's
+// transforms), so a block finds its item by binary search.
+template <bool DIF>
+__global__ void __launch_bounds__(512) k_ntt_pass_list(const NttPassItem *items, int n_items)
+{
+    extern __shared__ Fr sm[];
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= blockIdx.x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const NttPassItem it = items[lo];
+    ntt_pass_tile<DIF>(sm, it.data, it.s_lo, it.t, it.tw, it.pre, it.post, it.post_const,
+                       blockIdx.x - it.first_block);
+}
+
+// h = (a b - c) (g^n - 1)^-1 for many vectors in one launch (item i owns the
+// elements [first, first + n) of the grid-wide index space)
+__global__ void k_quotient_list(const QuotientItem *items, int n_items, uint64_t total)
+{
+    const uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const QuotientItem &it = items[lo];
+    const uint64_t i = g - it.first;
+    it.h[i] = (it.a[i] * it.b[i] - it.c[i]) * *it.zinv;
 }
 
 __global__ void k_bitrev_permute(const Fr *in, Fr *out, int logn, const Fr *scale,
@@ -221,6 +270,62 @@ int run_passes(const NttTables &tb, Fr *data, bool dif, bool inverse, const Fr *
             k_ntt_pass<false><<<blocks, threads, G * sizeof(Fr), st>>>(data, s_lo, t, tw, pr, po, pc);
         NKR_CHECK_LAUNCH();
         if (!dif) s_lo += t;
+    }
+    return NKR_B200_OK;
+}
+
+// The passes of several transforms, pass q of all of them in one launch.
+int run_list(const NttJob *jobs, int n_jobs, bool dif, bool inverse, NttPassItem *items_host,
+             NttPassItem *items_dev, cudaStream_t st)
+{
+    if (n_jobs <= 0) return NKR_B200_OK;
+    struct Plan {
+        int np, ts[8], s_lo;
+    };
+    std::vector<Plan> plans(n_jobs);
+    int max_np = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        const NttTables &tb = *jobs[j].tables;
+        plans[j].np = pass_plan(tb.logn, tb.max_stages, plans[j].ts);
+        plans[j].s_lo = dif ? tb.logn : 0;
+        max_np = std::max(max_np, plans[j].np);
+    }
+    NttPassItem *items = items_host;
+    std::vector<int> count(max_np, 0);
+    std::vector<uint32_t> blocks(max_np, 0), threads(max_np, 32), smem(max_np, 0);
+    for (int q = 0; q < max_np; ++q) {
+        for (int j = 0; j < n_jobs; ++j) {
+            Plan &pl = plans[j];
+            if (q >= pl.np) continue;
+            const NttTables &tb = *jobs[j].tables;
+            const int t = pl.ts[q];
+            if (dif) pl.s_lo -= t;
+            NttPassItem &it = items[size_t(q) * n_jobs + count[q]++];
+            it.data = jobs[j].data;
+            it.tw = inverse ? tb.tw_inv.as<Fr>() : tb.tw_fwd.as<Fr>();
+            it.pre = q == 0 ? jobs[j].pre : nullptr;
+            it.post = q == pl.np - 1 ? jobs[j].post : nullptr;
+            it.post_const = q == pl.np - 1 ? jobs[j].post_const : nullptr;
+            it.first_block = blocks[q];
+            it.s_lo = pl.s_lo;
+            it.t = t;
+            const uint64_t nb = tb.n >> t;
+            NKR_REQUIRE(uint64_t(blocks[q]) + nb < (uint64_t(1) << 31), "batched NTT pass too large");
+            blocks[q] += uint32_t(nb);
+            threads[q] = std::max(threads[q], pass_threads(t, tb.bfly_per_thread));
+            smem[q] = std::max<uint32_t>(smem[q], (1u << t) * uint32_t(sizeof(Fr)));
+            if (!dif) pl.s_lo += t;
+        }
+    }
+    NKR_CUDA(cudaMemcpyAsync(items_dev, items, size_t(max_np) * n_jobs * sizeof(NttPassItem),
+                             cudaMemcpyHostToDevice, st));
+    for (int q = 0; q < max_np; ++q) {
+        const NttPassItem *d = items_dev + size_t(q) * n_jobs;
+        if (dif)
+            k_ntt_pass_list<true><<<blocks[q], threads[q], smem[q], st>>>(d, count[q]);
+        else
+            k_ntt_pass_list<false><<<blocks[q], threads[q], smem[q], st>>>(d, count[q]);
+        NKR_CHECK_LAUNCH();
     }
     return NKR_B200_OK;
 }
@@ -328,6 +433,27 @@ int ntt_dit(const NttTables &t, Fr *data, bool inverse, const Fr *pre, const Fr 
             const Fr *post_const, cudaStream_t st)
 {
     return run_passes(t, data, false, inverse, pre, post, post_const, st);
+}
+
+int ntt_run_list(const NttJob *jobs, int n_jobs, bool dif, bool inverse, NttPassItem *items_host,
+                 NttPassItem *items_dev, cudaStream_t st)
+{
+    return run_list(jobs, n_jobs, dif, inverse, items_host, items_dev, st);
+}
+
+int fr_quotient_list(QuotientItem *items, int n_items, QuotientItem *items_dev, cudaStream_t st)
+{
+    if (n_items <= 0) return NKR_B200_OK;
+    uint64_t total = 0;
+    for (int i = 0; i < n_items; ++i) {
+        const uint64_t n = items[i].first; // on input: the item's length
+        items[i].first = total;
+        total += n;
+    }
+    NKR_CUDA(cudaMemcpyAsync(items_dev, items, n_items * sizeof(QuotientItem), cudaMemcpyHostToDevice, st));
+    k_quotient_list<<<blocks_for(total, 256), 256, 0, st>>>(items_dev, n_items, total);
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
 }
 
 int ntt_bitrev_permute(const Fr *in, Fr *out, uint64_t n, const Fr *scale, const Fr *scale_const,

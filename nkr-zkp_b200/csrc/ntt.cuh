@@ -69,6 +69,37 @@ int fr_scale_const(Fr *data, uint64_t n, const Fr *c, cudaStream_t st);
 int fr_quotient_pointwise(const Fr *a, const Fr *b, const Fr *c, Fr *h, uint64_t n,
                           const Fr *zinv, cudaStream_t st);
 
+// Transforms of several vectors (of any sizes, each with its own tables) run pass
+// by pass, every pass of all of them in one launch (a batch of proofs' quotient
+// chains).  The transforms in one call are independent; each item's passes are
+// those ntt_dif / ntt_dit would run for it.
+struct NttPassItem {
+    Fr *data;
+    const Fr *tw, *pre, *post, *post_const;
+    uint32_t first_block; // prefix over items of the blocks of this pass
+    int s_lo, t;
+};
+struct NttJob {
+    const NttTables *tables;
+    Fr *data;
+    const Fr *pre, *post, *post_const;
+};
+// items_host (pinned) and items_dev: 8 n_jobs items each (up to 8 passes); the
+// host items are read by the stream's copy, so they must stay untouched until the
+// stream has passed this call
+int ntt_run_list(const NttJob *jobs, int n_jobs, bool dif, bool inverse, NttPassItem *items_host,
+                 NttPassItem *items_dev, cudaStream_t st);
+
+// (a b - c) / Z(g) for several vectors in one launch
+struct QuotientItem {
+    const Fr *a, *b, *c;
+    Fr *h;
+    const Fr *zinv;
+    uint64_t first; // the caller passes each item's length; replaced by the prefix
+};
+// items_host: pinned, rewritten in place (lengths -> prefixes) and read by the copy
+int fr_quotient_list(QuotientItem *items_host, int n_items, QuotientItem *items_dev, cudaStream_t st);
+
 // Table pieces and the DIT transform over caller-owned device memory (nothing is
 // allocated; used by the allocation-free entry point).  The stage twiddle table
 // tw[2^s + k] = w_{2^(s+1)}^k does not depend on N, so one table built for 2^L

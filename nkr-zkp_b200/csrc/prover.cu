@@ -464,6 +464,283 @@ int admit_slots(nkr_b200_key *key, int want)
 
 } // namespace
 
+namespace {
+
+// One wave of a batch: at most one proof per prove slot, all proofs' stages
+// aligned so that the work of every proof in a stage runs as one launch over a
+// device work list.  Per proof (on its slot's streams): witness upload, SpMV,
+// the witness digit sorts; then, across the wave, the level-1 bucket
+// accumulation of every G1 witness MSM in one launch (stream bw) and of every
+// G2 MSM in another (stream bw2); per proof the fix-up and reduction levels.
+// Across the wave on stream bq: the quotient chains, each NTT pass of every
+// proof's transforms in one launch and the pointwise step of all proofs in one;
+// per proof the digit sort of H; the level-1 accumulation of every H MSM in one
+// launch; per proof the H MSM's remaining levels, the join of the witness MSMs
+// and the result download.
+struct WaveProof {
+    nkr_b200_key *key;
+    ProveSlot *slot;
+    const void *witness;
+    uint8_t *result; // pinned host, kOutBytes
+};
+
+struct WaveScratch {
+    cudaStream_t bq = nullptr, bw = nullptr, bw2 = nullptr; // chains + H, G1 witness, G2 witness
+    cudaEvent_t ev_wacc = nullptr, ev_wacc2 = nullptr, ev_chain = nullptr, ev_hacc = nullptr;
+    std::vector<cudaEvent_t> ev_ready, ev_hsort; // per proof and witness MSM / per proof
+    DevBuf ntt_items, q_items, w_items, h_items;
+    // pinned host staging of the work lists: three NTT lists, quotient, witness
+    // and H accumulation lists (the copies read it asynchronously)
+    uint8_t *stage = nullptr;
+    size_t ntt_bytes = 0, q_bytes = 0, w_bytes = 0, h_bytes = 0;
+    NttPassItem *stage_ntt(int call) { return reinterpret_cast<NttPassItem *>(stage + call * ntt_bytes); }
+    QuotientItem *stage_q() { return reinterpret_cast<QuotientItem *>(stage + 3 * ntt_bytes); }
+    uint8_t *stage_w() { return stage + 3 * ntt_bytes + q_bytes; }
+    uint8_t *stage_h() { return stage + 3 * ntt_bytes + q_bytes + w_bytes; }
+    ~WaveScratch()
+    {
+        if (stage) {
+            if (bq) cudaStreamSynchronize(bq);
+            if (bw) cudaStreamSynchronize(bw);
+            if (bw2) cudaStreamSynchronize(bw2);
+            cudaFreeHost(stage);
+        }
+        for (cudaStream_t st : {bq, bw, bw2})
+            if (st) {
+                cudaStreamSynchronize(st);
+                cudaStreamDestroy(st);
+            }
+        for (cudaEvent_t e : {ev_wacc, ev_wacc2, ev_chain, ev_hacc})
+            if (e) cudaEventDestroy(e);
+        for (auto e : ev_ready)
+            if (e) cudaEventDestroy(e);
+        for (auto e : ev_hsort)
+            if (e) cudaEventDestroy(e);
+    }
+    int init(size_t max_wave)
+    {
+        NKR_CUDA(cudaStreamCreateWithFlags(&bq, cudaStreamNonBlocking));
+        NKR_CUDA(cudaStreamCreateWithFlags(&bw, cudaStreamNonBlocking));
+        NKR_CUDA(cudaStreamCreateWithFlags(&bw2, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&ev_wacc, &ev_wacc2, &ev_chain, &ev_hacc})
+            NKR_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        ev_ready.assign(max_wave * 4, nullptr);
+        ev_hsort.assign(max_wave, nullptr);
+        for (auto &e : ev_ready) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto &e : ev_hsort) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ntt_bytes = 8 * 3 * max_wave * sizeof(NttPassItem);
+        q_bytes = max_wave * sizeof(QuotientItem);
+        w_bytes = 4 * max_wave * kMsmAccItemBytes;
+        h_bytes = max_wave * kMsmAccItemBytes;
+        NKR_TRY(ntt_items.alloc(ntt_bytes, "batch NTT work list"));
+        NKR_TRY(q_items.alloc(q_bytes, "batch quotient work list"));
+        NKR_TRY(w_items.alloc(w_bytes, "batch accumulation work list"));
+        NKR_TRY(h_items.alloc(h_bytes, "batch accumulation work list"));
+        if (cudaHostAlloc(reinterpret_cast<void **>(&stage), 3 * ntt_bytes + q_bytes + w_bytes + h_bytes,
+                          cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            stage = nullptr;
+            set_error("pinned work-list staging allocation failed");
+            return NKR_B200_ENOMEM;
+        }
+        return NKR_B200_OK;
+    }
+};
+
+int run_wave(const std::vector<WaveProof> &wave, WaveScratch &ws)
+{
+    const size_t P = wave.size();
+    // the previous wave's work-list copies have read the staging area
+    NKR_CUDA(cudaStreamSynchronize(ws.bq));
+    NKR_CUDA(cudaStreamSynchronize(ws.bw));
+    NKR_CUDA(cudaStreamSynchronize(ws.bw2));
+    // per proof: upload, SpMV, witness sorts
+    for (size_t p = 0; p < P; ++p) {
+        nkr_b200_key *key = wave[p].key;
+        ProveSlot *sl = wave[p].slot;
+        cudaStream_t s0 = sl->main();
+        NKR_TRY(slot_upload_witness(key, sl, wave[p].witness));
+        const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
+        Fr *ys[3] = {sl->az.as<Fr>(), sl->bz.as<Fr>(), sl->cz.as<Fr>()};
+        Fr *prods[3] = {sl->spmv_prod[0].as<Fr>(), sl->spmv_prod[1].as<Fr>(), sl->spmv_prod[2].as<Fr>()};
+        NKR_TRY(spmv_multi(mats, 3, sl->z.as<Fr>(), ys, prods, s0));
+        NKR_CUDA(cudaEventRecord(sl->ev_z, s0));
+        for (int g = 0; g < key->n_sorts; ++g) {
+            const int o = key->sort_stream[g];
+            NKR_CUDA(cudaStreamWaitEvent(sl->st[o], sl->ev_z, 0));
+            NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], sl->z.p, sl->st[o],
+                                 key->bases[o].gather()));
+            NKR_CUDA(cudaEventRecord(sl->ev_sorted[g], sl->st[o]));
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int k = kWitnessOrder[i];
+            const int g = key->sort_of[k];
+            if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(sl->st[k], sl->ev_sorted[g], 0));
+            NKR_CUDA(cudaEventRecord(ws.ev_ready[4 * p + i], sl->st[k]));
+        }
+    }
+    // witness MSMs: level 1 of the wave's G1 MSMs in one launch (stream bw) and of
+    // its G2 MSMs in another (stream bw2)
+    std::vector<MsmAccJob> g1, g2;
+    for (size_t p = 0; p < P; ++p) {
+        nkr_b200_key *key = wave[p].key;
+        ProveSlot *sl = wave[p].slot;
+        for (int i = 0; i < 4; ++i) {
+            const int k = kWitnessOrder[i];
+            const bool is_g1 = key->bases[k].group == 1;
+            NKR_CUDA(cudaStreamWaitEvent(is_g1 ? ws.bw : ws.bw2, ws.ev_ready[4 * p + i], 0));
+            MsmAccJob j{&key->bases[k], &sl->sort_w[key->sort_of[k]], &sl->acc[k]};
+            (is_g1 ? g1 : g2).push_back(j);
+        }
+    }
+    uint8_t *wi = ws.w_items.as<uint8_t>();
+    uint8_t *wh = ws.stage_w();
+    NKR_TRY(msm_acc_level1_list(1, g1.data(), int(g1.size()), wh, wi, ws.bw));
+    NKR_TRY(msm_acc_level1_list(2, g2.data(), int(g2.size()), wh + g1.size() * kMsmAccItemBytes,
+                                wi + g1.size() * kMsmAccItemBytes, ws.bw2));
+    NKR_CUDA(cudaEventRecord(ws.ev_wacc, ws.bw));
+    NKR_CUDA(cudaEventRecord(ws.ev_wacc2, ws.bw2));
+    for (size_t p = 0; p < P; ++p) {
+        nkr_b200_key *key = wave[p].key;
+        ProveSlot *sl = wave[p].slot;
+        uint8_t *out = sl->out.as<uint8_t>();
+        for (int k : kWitnessOrder) {
+            NKR_CUDA(cudaStreamWaitEvent(sl->st[k], key->bases[k].group == 1 ? ws.ev_wacc : ws.ev_wacc2, 0));
+            NKR_TRY(msm_acc_tail(key->bases[k], sl->sort_w[key->sort_of[k]], sl->acc[k],
+                                 out + kOutOffset[k], sl->st[k]));
+            NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
+        }
+    }
+    // quotient chains: every pass of every proof's transforms in one launch
+    std::vector<NttJob> jobs;
+    std::vector<QuotientItem> qi;
+    for (size_t p = 0; p < P; ++p) {
+        ProveSlot *sl = wave[p].slot;
+        NKR_CUDA(cudaStreamWaitEvent(ws.bq, sl->ev_z, 0));
+    }
+    NttPassItem *ni = ws.ntt_items.as<NttPassItem>();
+    for (size_t p = 0; p < P; ++p) {
+        const NttTables &T = wave[p].key->ntt;
+        ProveSlot *sl = wave[p].slot;
+        for (Fr *v : {sl->az.as<Fr>(), sl->bz.as<Fr>(), sl->cz.as<Fr>()})
+            jobs.push_back(NttJob{&T, v, nullptr, nullptr, nullptr});
+    }
+    NKR_TRY(ntt_run_list(jobs.data(), int(jobs.size()), true, true, ws.stage_ntt(0), ni, ws.bq)); // iFFT (DIF)
+    for (size_t p = 0; p < P; ++p)
+        for (int v = 0; v < 3; ++v) jobs[3 * p + v].pre = wave[p].key->ntt.t1.as<Fr>();
+    NKR_TRY(ntt_run_list(jobs.data(), int(jobs.size()), false, false, ws.stage_ntt(1), ni, ws.bq)); // cosetFFT
+    for (size_t p = 0; p < P; ++p) {
+        const NttTables &T = wave[p].key->ntt;
+        ProveSlot *sl = wave[p].slot;
+        qi.push_back(QuotientItem{sl->az.as<Fr>(), sl->bz.as<Fr>(), sl->cz.as<Fr>(), sl->h.as<Fr>(),
+                                  T.consts.as<Fr>() + kConstZinv, wave[p].key->rows});
+    }
+    std::copy(qi.begin(), qi.end(), ws.stage_q());
+    NKR_TRY(fr_quotient_list(ws.stage_q(), int(qi.size()), ws.q_items.as<QuotientItem>(), ws.bq));
+    jobs.clear();
+    for (size_t p = 0; p < P; ++p)
+        jobs.push_back(NttJob{&wave[p].key->ntt, wave[p].slot->h.as<Fr>(), nullptr,
+                              wave[p].key->ntt.t2.as<Fr>(), nullptr});
+    NKR_TRY(ntt_run_list(jobs.data(), int(jobs.size()), true, true, ws.stage_ntt(2), ni, ws.bq)); // icosetFFT
+    NKR_CUDA(cudaEventRecord(ws.ev_chain, ws.bq));
+    // H: per proof the sort, then level 1 of every H MSM in one launch
+    std::vector<MsmAccJob> hj;
+    for (size_t p = 0; p < P; ++p) {
+        nkr_b200_key *key = wave[p].key;
+        ProveSlot *sl = wave[p].slot;
+        cudaStream_t s0 = sl->main();
+        NKR_CUDA(cudaStreamWaitEvent(s0, ws.ev_chain, 0));
+        NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, sl->sort_h, sl->h.p, s0));
+        NKR_CUDA(cudaEventRecord(ws.ev_hsort[p], s0));
+        NKR_CUDA(cudaStreamWaitEvent(ws.bq, ws.ev_hsort[p], 0));
+        hj.push_back(MsmAccJob{&key->bases[kMsmH], &sl->sort_h, &sl->acc[kMsmH]});
+    }
+    NKR_TRY(msm_acc_level1_list(1, hj.data(), int(hj.size()), ws.stage_h(), ws.h_items.p, ws.bq));
+    NKR_CUDA(cudaEventRecord(ws.ev_hacc, ws.bq));
+    for (size_t p = 0; p < P; ++p) {
+        nkr_b200_key *key = wave[p].key;
+        ProveSlot *sl = wave[p].slot;
+        cudaStream_t s0 = sl->main();
+        NKR_CUDA(cudaStreamWaitEvent(s0, ws.ev_hacc, 0));
+        NKR_TRY(msm_acc_tail(key->bases[kMsmH], sl->sort_h, sl->acc[kMsmH],
+                             sl->out.as<uint8_t>() + kOutOffset[kMsmH], s0));
+        for (int k : kWitnessOrder) NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_done[k], 0));
+        NKR_CUDA(cudaMemcpyAsync(wave[p].result, sl->out.p, kOutBytes, cudaMemcpyDeviceToHost, s0));
+    }
+    return NKR_B200_OK;
+}
+
+} // namespace
+
+int key_prove_batch_lists(nkr_b200_key *const *keys, const void *const *witnesses, int count,
+                          nkr_b200_raw_proof *out)
+{
+    NKR_REQUIRE(keys && witnesses && out && count >= 0, "null argument");
+    if (count == 0) return NKR_B200_OK;
+    std::vector<nkr_b200_key *> distinct;
+    std::vector<int> per_key;
+    for (int i = 0; i < count; ++i) {
+        NKR_REQUIRE(keys[i] && witnesses[i], "null key or witness at %d", i);
+        NKR_REQUIRE(keys[i]->ctx == keys[0]->ctx, "batch keys belong to different contexts");
+        size_t j = 0;
+        while (j < distinct.size() && distinct[j] != keys[i]) ++j;
+        if (j == distinct.size()) {
+            distinct.push_back(keys[i]);
+            per_key.push_back(0);
+        }
+        ++per_key[j];
+    }
+    NKR_CUDA(cudaSetDevice(keys[0]->ctx->device));
+    size_t max_wave = 0;
+    for (size_t j = 0; j < distinct.size(); ++j) {
+        NKR_TRY(admit_slots(distinct[j], std::min(per_key[j], kMaxSlotsPerKey)));
+        max_wave += distinct[j]->slots.size();
+    }
+    max_wave = std::min<size_t>(max_wave, size_t(count));
+    void *res = nullptr;
+    if (cudaHostAlloc(&res, size_t(count) * kOutBytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("pinned result allocation failed");
+        return NKR_B200_ENOMEM;
+    }
+    int status = NKR_B200_OK;
+    {
+        WaveScratch ws;
+        status = ws.init(max_wave);
+        // waves: proofs in order, each on the next free slot of its key; a proof
+        // whose key has no free slot left starts the next wave
+        std::vector<WaveProof> wave;
+        std::vector<size_t> used(distinct.size(), 0);
+        for (int i = 0; i < count && status == NKR_B200_OK; ++i) {
+            const size_t j = size_t(std::find(distinct.begin(), distinct.end(), keys[i]) - distinct.begin());
+            if (used[j] == distinct[j]->slots.size()) {
+                status = run_wave(wave, ws);
+                wave.clear();
+                std::fill(used.begin(), used.end(), size_t(0));
+            }
+            if (status != NKR_B200_OK) break;
+            wave.push_back(WaveProof{keys[i], distinct[j]->slots[used[j]++].get(), witnesses[i],
+                                     static_cast<uint8_t *>(res) + size_t(i) * kOutBytes});
+        }
+        if (status == NKR_B200_OK && !wave.empty()) status = run_wave(wave, ws);
+        for (auto *key : distinct)
+            for (auto &sl : key->slots)
+                for (auto st : sl->st)
+                    if (cudaStreamSynchronize(st) != cudaSuccess && status == NKR_B200_OK) {
+                        set_error("batch: %s", cudaGetErrorString(cudaGetLastError()));
+                        status = NKR_B200_ECUDA;
+                    }
+    }
+    if (status == NKR_B200_OK)
+        for (int i = 0; i < count; ++i) {
+            uint8_t *o = static_cast<uint8_t *>(res) + size_t(i) * kOutBytes;
+            normalize_raw(o);
+            raw_from_bytes(o, &out[i]);
+        }
+    cudaFreeHost(res);
+    return status;
+}
+
 int key_prove_batch(nkr_b200_key *const *keys, const void *const *witnesses, int count,
                     nkr_b200_raw_proof *out)
 {

@@ -106,6 +106,8 @@ _SIGS = {
     "nkr_b200_key_stage_times": (ctypes.c_int, [_VP, ctypes.POINTER(StageTimes)]),
     "nkr_b200_prove_batch": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
                                             ctypes.POINTER(RawProofC)]),
+    "nkr_b200_prove_batch_lists": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.c_int,
+                                            ctypes.POINTER(RawProofC)]),
     "nkr_b200_ntt": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _U64]),
     "nkr_b200_tune_ntt": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int)]),
@@ -613,9 +615,10 @@ def write_proving_key(path, pk, rows, cols):
            "nkr_b200_write_proving_key")
 
 
-def prove_batch(backends, witnesses=None, witness_ptrs=None):
-    """Batched prove (nkr_b200_prove_batch): numpy witnesses, or raw pointers
-    (pinned host or device memory) in witness_ptrs."""
+def prove_batch(backends, witnesses=None, witness_ptrs=None, lists=False):
+    """Batched prove (nkr_b200_prove_batch, or nkr_b200_prove_batch_lists with
+    cross-proof launches when lists): numpy witnesses, or raw pointers (pinned
+    host or device memory) in witness_ptrs."""
     n = len(backends)
     keys = (_VP * n)(*[b.key for b in backends])
     if witness_ptrs is None:
@@ -623,7 +626,8 @@ def prove_batch(backends, witnesses=None, witness_ptrs=None):
         witness_ptrs = [w.ctypes.data for w in ws]
     wp = (_VP * n)(*witness_ptrs)
     out = (RawProofC * n)()
-    _check(_lib.nkr_b200_prove_batch(keys, wp, n, out), "prove_batch")
+    f = _lib.nkr_b200_prove_batch_lists if lists else _lib.nkr_b200_prove_batch
+    _check(f(keys, wp, n, out), "prove_batch")
     return list(out)
 
 

@@ -145,6 +145,17 @@ def test_batch_mix_equals_single_proves(ctx):
     # a second batch reuses the captured graphs and slots
     out2 = nk.prove_batch([backends[j] for j, _ in order], [wits[j][i] for j, i in order])
     assert [bytes(r) for r in out2] == [bytes(r) for r in out]
+    # cross-proof launches (work lists over the proofs of a wave; 6 proofs of one
+    # key over its 4 slots make two waves): the same raw proofs
+    out3 = nk.prove_batch([backends[j] for j, _ in order], [wits[j][i] for j, i in order],
+                          lists=True)
+    for (j, i), raw in zip(order, out3):
+        assert bytes(raw) == single[j][i], f"lists: key {j} witness {i}"
+    # and in a different order, the first proofs of each key in the last wave
+    rev = order[::-1]
+    out4 = nk.prove_batch([backends[j] for j, _ in rev], [wits[j][i] for j, i in rev], lists=True)
+    for (j, i), raw in zip(rev, out4):
+        assert bytes(raw) == single[j][i], f"lists, reversed: key {j} witness {i}"
     for be in backends:
         be.free()
 
