@@ -15,8 +15,10 @@ of a fresh seeded witness on resident keys.
   e2e       the same through the C ABI from pinned host memory: witness upload,
             prove, raw-proof download, blinding with seeded r, s, proof download.
   roofline  the dominant kernel (MSM bucket accumulation) in Fq-multiplications/s
-            against this GPU's measured Montgomery-product throughput; HBM bytes
-            of the same kernel against the measured copy bandwidth beside it.
+            against the instruction-issue ceiling of the product (SMs x 4 warp
+            instructions per cycle x 32 lanes x SM clock / instructions per
+            product); HBM bytes of the same kernel against the measured copy
+            bandwidth beside it.
   cpu_baseline  one single-threaded prove of the same circuit, key and witness by
             the reference's own CPU prover (oracle/_ref: libff/libfqfft built from
             the reference sources, one thread as the reference's bench runs it),
@@ -511,7 +513,13 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank != 0:
         return
-    s_med = {k: round(statistics.median(s[k] for s in stage), 3) for k in stage[0]}
+    s_med = {k: round(statistics.median(s[k] for s in stage), 3) for k in stage[0]
+             if not k.endswith(("_start_ms", "l1_end_ms", "fixup_end_ms", "reduce_first_end_ms"))}
+    # each MSM's phases in the concurrent prove: level-1 start / end, fix-ups end,
+    # first reduction level end, MSM end (ms from the prove's start)
+    timeline = {m: [round(statistics.median(s[f"msm_{m}_{ph}_ms"] for s in stage), 3)
+                    for ph in ("l1_start", "l1_end", "fixup_end", "reduce_first_end", "end")]
+                for m in ("a", "b_g1", "b_g2", "l", "h")}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -523,6 +531,8 @@ def run_b200(args):
         "config": _config(kind, param, dens, r1.rows, r1.cols, world),
         "key_device_gib": round(key_gb, 2),
         "stages_ms_median": s_med,
+        "msm_timeline_ms_median": {"phases": ["l1_start", "l1_end", "fixup_end",
+                                              "reduce_first_end", "end"], **timeline},
         "prepare_ms": {"first": round(prep_ms[0], 1),
                        "tuned": round(statistics.median(prep_ms[1:]), 1)},
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d,

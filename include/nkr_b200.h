@@ -104,6 +104,10 @@ typedef struct {
 typedef struct {
     float spmv_ms, quotient_ms, witness_msms_ms, quotient_msm_ms, total_ms;
     float msm_a_end_ms, msm_b_g1_end_ms, msm_b_g2_end_ms, msm_l_end_ms, msm_h_end_ms;
+    /* per MSM (A, B_G1, B_G2, L, H), ms from the start of the prove: start and end
+     * of the level-1 bucket accumulation, end of the fix-up levels, end of the
+     * first reduction level (the MSM ends at msm_*_end_ms) */
+    float msm_phase_ms[5][4];
 } nkr_b200_stage_times;
 
 /* ---- context -------------------------------------------------------------- */

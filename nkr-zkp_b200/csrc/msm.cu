@@ -133,6 +133,20 @@ struct MsmArith<Fq2> {
 template <class F>
 using CF = typename MsmArith<F>::type;
 
+// Compute type of the bucket reduction levels (first level, block levels, final
+// combination): latency-bound chains of dependent additions, where G2 gains from
+// the lazily reduced Fq2 product (Fq2L, field.cuh).
+template <class F>
+struct MsmReduceArith {
+    using type = CF<F>;
+};
+template <>
+struct MsmReduceArith<Fq2> {
+    using type = Fq2L;
+};
+template <class F>
+using CR = typename MsmReduceArith<F>::type;
+
 __device__ __forceinline__ Fq52 msm_in(const Fq &x) { return to52(x); }
 __device__ __forceinline__ Fq msm_out(const Fq52 &x) { return from52(x); }
 __device__ __forceinline__ Fq52 msm_enter(const Fq52 &x) { return r256_to_r260(x); }
@@ -144,6 +158,12 @@ __device__ __forceinline__ Fq2 msm_leave(const Fq2 &x) { return x; }
 
 template <class F>
 __device__ __forceinline__ Xyzz<CF<F>> ldx(const Xyzz<F> &s)
+{
+    return {msm_in(s.x), msm_in(s.y), msm_in(s.zz), msm_in(s.zzz)};
+}
+
+template <class F>
+__device__ __forceinline__ Xyzz<CR<F>> ldr(const Xyzz<F> &s)
 {
     return {msm_in(s.x), msm_in(s.y), msm_in(s.zz), msm_in(s.zzz)};
 }
@@ -407,7 +427,7 @@ int first_level_log2(uint32_t m, int log2_bs)
 // (one piece) or by the fix-up levels (more than kSmallPieces pieces), or else
 // its few pieces are added straight from the partial slots.
 template <class F>
-__device__ __forceinline__ Xyzz<CF<F>> add_bucket_sum(Xyzz<CF<F>> run,
+__device__ __forceinline__ Xyzz<CR<F>> add_bucket_sum(Xyzz<CR<F>> run,
                                                       const uint32_t *__restrict__ offsets,
                                                       const Xyzz<F> *__restrict__ partials,
                                                       const Xyzz<F> *__restrict__ buckets, uint32_t b,
@@ -416,8 +436,8 @@ __device__ __forceinline__ Xyzz<CF<F>> add_bucket_sum(Xyzz<CF<F>> run,
     const uint32_t lo = offsets[b], hi = offsets[b + 1];
     if (hi == lo) return run;
     const Pieces pc{lo / k1, (hi - 1) / k1 - lo / k1 + 1};
-    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldx(buckets[b]));
-    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldx(partials[pc.slot(lo, k1, k)]));
+    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldr(buckets[b]));
+    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldr(partials[pc.slot(lo, k1, k)]));
     return run;
 }
 
@@ -436,7 +456,7 @@ __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict
     const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t * L >= items) return;
     const uint64_t base = t * L;
-    Xyzz<CF<F>> run = Xyzz<CF<F>>::inf(), tri = Xyzz<CF<F>>::inf();
+    Xyzz<CR<F>> run = Xyzz<CR<F>>::inf(), tri = Xyzz<CR<F>>::inf();
     for (int i = int(L) - 1; i >= 0; --i) {
         run = add_bucket_sum(run, offsets, partials, buckets, uint32_t(base + i), k1);
         if (i > 0) tri = xyzz_add(tri, run);
@@ -461,7 +481,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
                                                       Xyzz<F> *__restrict__ a_out,
                                                       Xyzz<F> *__restrict__ r_out)
 {
-    using C = CF<F>;
+    using C = CR<F>;
     extern __shared__ uint8_t smem_raw[];
     Xyzz<C> *buf0 = reinterpret_cast<Xyzz<C> *>(smem_raw);
     Xyzz<C> *buf1 = buf0 + BS;
@@ -472,7 +492,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     const uint64_t idx = uint64_t(blk) * BS + i;
     const bool live = idx < m;
     const uint64_t g = uint64_t(set) * m + idx;
-    Xyzz<C> v = live ? ldx(r_in[g]) : Xyzz<C>::inf();
+    Xyzz<C> v = live ? ldr(r_in[g]) : Xyzz<C>::inf();
     buf0[i] = v;
     __syncthreads();
     Xyzz<C> *cur = buf0, *nxt = buf1;
@@ -488,7 +508,7 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     const Xyzz<C> total = cur[0];
     __syncthreads();
     buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
-    buf1[i] = (a_in && live) ? ldx(a_in[g]) : Xyzz<C>::inf();
+    buf1[i] = (a_in && live) ? ldr(a_in[g]) : Xyzz<C>::inf();
     __syncthreads();
     // the two tree sums run side by side on disjoint threads (first s: weighted
     // suffix sums, next s: A items), one addition per thread and step
@@ -514,9 +534,9 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
 // X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point; the
 // coordinates leave the R' domain here (back to the library's R = 2^256).
 template <class F>
-__device__ __forceinline__ void store_jacobian(const Xyzz<CF<F>> &p, F *out)
+__device__ __forceinline__ void store_jacobian(const Xyzz<CR<F>> &p, F *out)
 {
-    using C = CF<F>;
+    using C = CR<F>;
     if (p.is_inf()) {
         out[0] = F::zero();
         out[1] = F::one();
@@ -534,12 +554,12 @@ template <class F>
 __global__ void k_finalize(const Xyzz<F> *a, const Xyzz<F> *r, int sets, int c, F *out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    using C = CF<F>;
+    using C = CR<F>;
     Xyzz<C> acc = Xyzz<C>::inf();
     for (int k = sets - 1; k >= 0; --k) {
         if (k != sets - 1)
             for (int d = 0; d < c; ++d) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, a ? xyzz_add(ldx(a[k]), ldx(r[k])) : ldx(r[k]));
+        acc = xyzz_add(acc, a ? xyzz_add(ldr(a[k]), ldr(r[k])) : ldr(r[k]));
     }
     store_jacobian<F>(acc, out);
 }
@@ -779,7 +799,7 @@ int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, c
     Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
     constexpr int BS = sizeof(F) == sizeof(Fq) ? 256 : 128; // G1: 256 buckets per block, G2: 128
     constexpr int kLog2BS = BS == 256 ? 8 : 7;
-    const size_t smem = 2 * BS * sizeof(Xyzz<CF<F>>);
+    const size_t smem = 2 * BS * sizeof(Xyzz<CR<F>>);
     NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
     // first level: bucket sums (few-piece buckets finished here), L buckets per thread

@@ -78,6 +78,9 @@ ProveSlot::~ProveSlot()
         if (e) cudaEventDestroy(e);
     for (auto e : ev_msm_end)
         if (e) cudaEventDestroy(e);
+    for (auto &a : acc)
+        for (auto e : a.ev_acc)
+            if (e) cudaEventDestroy(e);
     for (auto p : pinned_wit)
         if (p) cudaFreeHost(p);
     if (pinned_out) cudaFreeHost(pinned_out);
@@ -123,6 +126,8 @@ int slot_add(nkr_b200_key *key)
     for (auto &e : sl->ev_wit) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : sl->ev_t) NKR_CUDA(cudaEventCreate(&e));
     for (auto &e : sl->ev_msm_end) NKR_CUDA(cudaEventCreate(&e));
+    for (auto &a : sl->acc)
+        for (auto &e : a.ev_acc) NKR_CUDA(cudaEventCreate(&e));
     size_t bytes = 0;
     for (int g = 0; g < key->n_sorts; ++g) {
         NKR_TRY(msm_sort_alloc(sl->sort_w[g], key->bases[key->sort_stream[g]].shape));
@@ -169,6 +174,7 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
     Fr *az = sl->az.as<Fr>(), *bz = sl->bz.as<Fr>(), *cz = sl->cz.as<Fr>(), *h = sl->h.as<Fr>();
     uint8_t *out = sl->out.as<uint8_t>();
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[0], s0));
+    for (auto &a : sl->acc) a.timing = timed; // phase events of each MSM (timed proves only)
     const CsrDevice *mats[3] = {&key->mat[0], &key->mat[1], &key->mat[2]};
     Fr *ys[3] = {az, bz, cz};
     Fr *prods[3] = {sl->spmv_prod[0].as<Fr>(), sl->spmv_prod[1].as<Fr>(), sl->spmv_prod[2].as<Fr>()};
@@ -416,6 +422,12 @@ int key_prove(nkr_b200_key *key, const void *witness, uint64_t n, nkr_b200_raw_p
     ends[kMsmH] = &key->times.msm_h_end_ms;
     for (int k = 0; k < kNumMsm; ++k)
         NKR_CUDA(cudaEventElapsedTime(ends[k], sl->ev_t[0], sl->ev_msm_end[k]));
+    // phases in the public MSM order A, B_G1, B_G2, L, H
+    const int order[kNumMsm] = {kMsmA, kMsmB1, kMsmB2, kMsmL, kMsmH};
+    for (int i = 0; i < kNumMsm; ++i)
+        for (int j = 0; j < 4; ++j)
+            NKR_CUDA(cudaEventElapsedTime(&key->times.msm_phase_ms[i][j], sl->ev_t[0],
+                                          sl->acc[order[i]].ev_acc[j]));
     key->have_times = true;
     return NKR_B200_OK;
 }

@@ -65,7 +65,11 @@ class StageTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in
                 ("spmv_ms", "quotient_ms", "witness_msms_ms", "quotient_msm_ms", "total_ms",
                  "msm_a_end_ms", "msm_b_g1_end_ms", "msm_b_g2_end_ms", "msm_l_end_ms",
-                 "msm_h_end_ms")]
+                 "msm_h_end_ms")] + [("msm_phase_ms", ctypes.c_float * 20)]
+
+
+_MSM_NAMES = ("a", "b_g1", "b_g2", "l", "h")
+_PHASE_NAMES = ("l1_start", "l1_end", "fixup_end", "reduce_first_end")
 
 
 class MsmStats(ctypes.Structure):
@@ -540,7 +544,11 @@ class Backend:
     def stage_times(self):
         t = StageTimes()
         _check(_lib.nkr_b200_key_stage_times(self.key, ctypes.byref(t)), "stage_times")
-        return {n: getattr(t, n) for n, _ in StageTimes._fields_}
+        out = {n: getattr(t, n) for n, _ in StageTimes._fields_ if n != "msm_phase_ms"}
+        for i, m in enumerate(_MSM_NAMES):
+            for j, ph in enumerate(_PHASE_NAMES):
+                out[f"msm_{m}_{ph}_ms"] = t.msm_phase_ms[4 * i + j]
+        return out
 
     def device_bytes(self):
         return int(_lib.nkr_b200_key_device_bytes(self.key))
