@@ -1057,6 +1057,11 @@ int msm_acc_level1_list(int group, const MsmAccJob *jobs, int n, void *items_hos
                       : acc_level1_list_t<Fq2>(jobs, n, items_host, items_dev, st);
 }
 
+int msm_acc_level1(const MsmBases &b, const MsmSort &s, MsmAcc &a, cudaStream_t st)
+{
+    return b.group == 1 ? acc_level1_t<Fq>(b, s, a, st) : acc_level1_t<Fq2>(b, s, a, st);
+}
+
 int msm_acc_tail(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
     return b.group == 1 ? acc_tail_t<Fq>(b, s, a, out_dev, st) : acc_tail_t<Fq2>(b, s, a, out_dev, st);

@@ -159,5 +159,7 @@ constexpr size_t kMsmAccItemBytes = 64; // scratch per job of msm_acc_level1_lis
 int msm_acc_level1_list(int group, const MsmAccJob *jobs, int n, void *items_host, void *items_dev,
                         cudaStream_t st);
 int msm_acc_tail(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st);
+// the level-1 kernel of msm_acc_run alone (msm_acc_tail finishes the MSM)
+int msm_acc_level1(const MsmBases &b, const MsmSort &s, MsmAcc &a, cudaStream_t st);
 
 } // namespace nkr

@@ -66,11 +66,17 @@ ProveSlot::~ProveSlot()
         if (s) cudaStreamSynchronize(s);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
+    for (auto s : tail)
+        if (s) cudaStreamSynchronize(s);
+    if (chain) cudaStreamSynchronize(chain);
     for (int k = 0; k < kNumMsm; ++k) {
         if (st[k]) cudaStreamDestroy(st[k]);
+        if (tail[k]) cudaStreamDestroy(tail[k]);
         if (ev_done[k]) cudaEventDestroy(ev_done[k]);
+        if (ev_l1[k]) cudaEventDestroy(ev_l1[k]);
     }
-    for (cudaEvent_t e : {ev_z, ev_wit[0], ev_wit[1]})
+    if (chain) cudaStreamDestroy(chain);
+    for (cudaEvent_t e : {ev_z, ev_wit[0], ev_wit[1], ev_hsorted})
         if (e) cudaEventDestroy(e);
     for (auto e : ev_sorted)
         if (e) cudaEventDestroy(e);
@@ -109,18 +115,26 @@ int slot_add(nkr_b200_key *key)
     NKR_CUDA(cudaSetDevice(key->ctx->device));
     auto slot = std::make_unique<ProveSlot>();
     ProveSlot *sl = slot.get();
-    // one priority for all streams of a slot: a higher priority for the main
-    // stream alone was measured slower (the H chain finishes early but the H MSM
-    // then crowds out the witness MSMs), and one or two levels more for the G2
-    // MSM's stream, the longest of a prove, ends it at 12.0 instead of 19.8 ms
-    // of a 2^20 prove while the other streams end later (20.05 vs 19.98 ms), and the
-    // quotient chain alone on a stream one or two levels higher ends at 6.1 instead
-    // of 14.8 ms while the witness MSMs end 4 ms later (20.7 ms)
+    // One priority for all streams of a slot.  Measured on a 2^20 prove (19.6 ms):
+    // a higher priority for the main stream alone is slower (the H chain finishes
+    // early but the H MSM then crowds out the witness MSMs); one or two levels more
+    // for the G2 MSM's stream end it at 12.0 instead of 19.8 ms while the others end
+    // later (20.05 vs 19.98 ms); the quotient chain one or two levels higher ends at
+    // 6.4 instead of 14.8 ms but the prove takes 20.2-20.6 ms (the level-1 kernels of
+    // several MSMs then share the SMs and all finish later); the fix-up and reduction
+    // levels one or two levels higher finish early but take SM slots from the level-1
+    // kernels (20.1-20.2 ms).  Running the level-1 kernels one after another on one
+    // stream, in any order, with or without waiting for the quotient chain, took
+    // 20.2-22.4 ms.
     const int prio = slot_stream_priority(key->logn);
     for (int k = 0; k < kNumMsm; ++k) {
         NKR_CUDA(cudaStreamCreateWithPriority(&sl->st[k], cudaStreamNonBlocking, prio));
+        NKR_CUDA(cudaStreamCreateWithPriority(&sl->tail[k], cudaStreamNonBlocking, prio));
         NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_done[k], cudaEventDisableTiming));
+        NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_l1[k], cudaEventDisableTiming));
     }
+    NKR_CUDA(cudaStreamCreateWithPriority(&sl->chain, cudaStreamNonBlocking, prio));
+    NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_hsorted, cudaEventDisableTiming));
     NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_z, cudaEventDisableTiming));
     for (auto &e : sl->ev_sorted) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : sl->ev_wit) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -189,32 +203,48 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
         NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], z, sl->st[o], key->bases[o].gather()));
         NKR_CUDA(cudaEventRecord(sl->ev_sorted[g], sl->st[o]));
     }
+    // level 1 on the MSM's stream, the fix-up and reduction levels on its tail stream
+    auto msm_issue = [&](int k, const MsmSort &so, cudaStream_t s_l1) -> int {
+        NKR_TRY(msm_acc_level1(key->bases[k], so, sl->acc[k], s_l1));
+        NKR_CUDA(cudaEventRecord(sl->ev_l1[k], s_l1));
+        NKR_CUDA(cudaStreamWaitEvent(sl->tail[k], sl->ev_l1[k], 0));
+        NKR_TRY(msm_acc_tail(key->bases[k], so, sl->acc[k], out + kOutOffset[k], sl->tail[k]));
+        if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[k], sl->tail[k]));
+        NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->tail[k]));
+        return NKR_B200_OK;
+    };
+    // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
+    auto chain_issue = [&]() -> int {
+        const NttTables &T = key->ntt;
+        const Fr *cst = T.consts.as<Fr>();
+        cudaStream_t sc = sl->chain;
+        NKR_CUDA(cudaStreamWaitEvent(sc, sl->ev_z, 0));
+        for (Fr *v : {az, bz, cz}) {
+            NKR_TRY(ntt_dif(T, v, true, nullptr, nullptr, nullptr, sc));
+            NKR_TRY(ntt_dit(T, v, false, T.t1.as<Fr>(), nullptr, nullptr, sc));
+        }
+        NKR_TRY(fr_quotient_pointwise(az, bz, cz, h, rows, cst + kConstZinv, sc));
+        NKR_TRY(ntt_dif(T, h, true, nullptr, T.t2.as<Fr>(), nullptr, sc));
+        if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[2], sc));
+        NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, sl->sort_h, h, sc));
+        NKR_CUDA(cudaEventRecord(sl->ev_hsorted, sc));
+        return NKR_B200_OK;
+    };
     for (int k : kWitnessOrder) {
         const int g = key->sort_of[k];
         if (key->sort_stream[g] != k) NKR_CUDA(cudaStreamWaitEvent(sl->st[k], sl->ev_sorted[g], 0));
-        NKR_TRY(msm_acc_run(key->bases[k], sl->sort_w[g], sl->acc[k], out + kOutOffset[k], sl->st[k]));
-        if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[k], sl->st[k]));
-        NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->st[k]));
+        NKR_TRY(msm_issue(k, sl->sort_w[g], sl->st[k]));
     }
-    // ar and bs1 tabulated for the blinding, behind the H chain on A's stream
+    NKR_TRY(chain_issue());
+    NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_hsorted, 0));
+    NKR_TRY(msm_issue(kMsmH, sl->sort_h, s0));
+    // ar and bs1 tabulated for the blinding, behind both MSMs on A's tail stream
     if (blind_tables) {
-        NKR_CUDA(cudaStreamWaitEvent(sl->st[kMsmA], sl->ev_done[kMsmB1], 0));
-        NKR_TRY(glv_tables_issue(sl, sl->st[kMsmA]));
-        NKR_CUDA(cudaEventRecord(sl->ev_done[kMsmA], sl->st[kMsmA]));
+        NKR_CUDA(cudaStreamWaitEvent(sl->tail[kMsmA], sl->ev_done[kMsmB1], 0));
+        NKR_TRY(glv_tables_issue(sl, sl->tail[kMsmA]));
+        NKR_CUDA(cudaEventRecord(sl->ev_done[kMsmA], sl->tail[kMsmA]));
     }
-    // H = icosetFFT((cosetFFT(iFFT(a)) * cosetFFT(iFFT(b)) - cosetFFT(iFFT(c))) / Z(g))
-    const NttTables &T = key->ntt;
-    const Fr *cst = T.consts.as<Fr>();
-    for (Fr *v : {az, bz, cz}) {
-        NKR_TRY(ntt_dif(T, v, true, nullptr, nullptr, nullptr, s0));
-        NKR_TRY(ntt_dit(T, v, false, T.t1.as<Fr>(), nullptr, nullptr, s0));
-    }
-    NKR_TRY(fr_quotient_pointwise(az, bz, cz, h, rows, cst + kConstZinv, s0));
-    NKR_TRY(ntt_dif(T, h, true, nullptr, T.t2.as<Fr>(), nullptr, s0));
-    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[2], s0));
-    NKR_TRY(msm_sort_run(key->bases[kMsmH].shape, sl->sort_h, h, s0));
-    NKR_TRY(msm_acc_run(key->bases[kMsmH], sl->sort_h, sl->acc[kMsmH], out + kOutOffset[kMsmH], s0));
-    if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[kMsmH], s0));
+    NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_done[kMsmH], 0));
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[3], s0));
     for (int k : kWitnessOrder) NKR_CUDA(cudaStreamWaitEvent(s0, sl->ev_done[k], 0));
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[4], s0));
@@ -226,6 +256,8 @@ int slot_capture(nkr_b200_key *key, ProveSlot *sl)
     if (sl->graph_exec) return NKR_B200_OK;
     NKR_CUDA(cudaSetDevice(key->ctx->device));
     for (auto s : sl->st) NKR_CUDA(cudaStreamSynchronize(s));
+    for (auto s : sl->tail) NKR_CUDA(cudaStreamSynchronize(s));
+    NKR_CUDA(cudaStreamSynchronize(sl->chain));
     cudaStream_t s0 = sl->main();
     const unsigned long long before = g_kernel_launches.load();
     NKR_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));

@@ -59,6 +59,11 @@ struct ProveSlot {
     DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
     DevBuf glv_tab; // slot 0: ar and bs1 of its last prove, tabulated for blinding (blind.cu)
     cudaStream_t st[kNumMsm] = {};
+    // higher-priority streams: each MSM's fix-up and reduction levels (tail[k]),
+    // and the quotient chain with the H digit sort (chain)
+    cudaStream_t tail[kNumMsm] = {};
+    cudaStream_t chain = nullptr;
+    cudaEvent_t ev_l1[kNumMsm] = {}, ev_hsorted = nullptr;
     cudaEvent_t ev_z = nullptr, ev_sorted[4] = {}, ev_done[kNumMsm] = {};
     cudaEvent_t ev_t[5] = {};
     cudaEvent_t ev_msm_end[kNumMsm] = {}; // timed proves: each MSM's end on its stream
