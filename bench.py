@@ -56,9 +56,9 @@ METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
 # DRAM read + write bytes per (point, digit) entry of the G1 accumulation kernel,
 # from an ncu capture at 2^18 points (a 2^20 capture would hold ~6 GB of keys on
 # the device); traffic grows with entries (one random base gather per entry)
-TRAFFIC_PER_ENTRY = (449.213184e6 + 22.324480e6) / 3932125   # 119.9 B per entry
+TRAFFIC_PER_ENTRY = (439.725568e6 + 21.505024e6) / 3932125   # 117.3 B per entry
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_acc_l1_g1 on the "
-                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 119.9 B "
+                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 117.3 B "
                   "per entry, scaled by this launch's entries")
 # Thread instructions per 52-bit-limb Fq product: ncu smsp__inst_executed.sum x 32 over
 # the products of nkr_b200_bench_mul's FP64 form (7,027,636,736 warp instructions for
@@ -66,10 +66,10 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_acc_l1_
 INSTR_PER_PRODUCT = 7027636736 * 32 / 620756992   # 362.3
 # Pipe counters of k_acc_l1_g1 from one ncu launch (2^18-point uniform G1 MSM of
 # --mode kernels; profiles/k_acc_l1_g1_msm_2_18.md); percentages of peak.
-ACC_NCU = {"issue_active_pct": 59.34, "fp64_pipe_pct": 40.79, "alu_pipe_pct": 52.55,
-           "fmaheavy_pipe_pct": 22.86, "warps_active_per_sm": 10.67, "registers": 168,
-           "stall_per_issue": {"wait": 0.83, "not_selected": 0.76, "math_pipe_throttle": 0.63,
-                               "long_scoreboard": 0.57},
+ACC_NCU = {"issue_active_pct": 58.83, "fp64_pipe_pct": 41.23, "alu_pipe_pct": 53.02,
+           "fmaheavy_pipe_pct": 20.13, "warps_active_per_sm": 10.69, "registers": 168,
+           "stall_per_issue": {"wait": 0.80, "not_selected": 0.76, "math_pipe_throttle": 0.67,
+                               "long_scoreboard": 0.55},
            "source": "ncu --metrics ... -k regex:k_acc_l1_g1 -c 1, --clock-control none"}
 
 

@@ -293,12 +293,126 @@ __device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets
         partials[2ull * t + (first ? 0 : 1)] = stx(acc);
 }
 
-// Level 1 kernels.  G1 (FP64 field, paired products passed by value) gets a
-// 3-blocks-per-SM register budget: measured against the compiler's own choice
-// (184 registers, 2 blocks) and a 4-block budget (128 registers, more spills),
-// it is the fastest from 2^16 to 2^20 points, uniform and sparse.  G2 keeps the
-// compiler's choice (232 registers, 2 blocks per SM; a 3-block budget spills 284 B
-// per thread and is no faster).
+// G1 level 1 with the accumulator in shared memory.  Across the out-of-line
+// product calls of a mixed addition the four accumulator coordinates were live
+// in registers (40 of the 168 the 3-blocks-per-SM budget allows); kept in
+// shared memory and loaded where a product needs them, they leave registers
+// for a 4-blocks-per-SM budget.  Layout: structure of arrays, word w of thread
+// i at w * BS + i, so a warp's 64-bit accesses are conflict-free.
+template <int BS>
+struct SmXyzz52 {
+    uint64_t *s; // the block's area + threadIdx.x
+    __device__ __forceinline__ Fq52 ld(int f) const
+    {
+        Fq52 v;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) v.l[j] = s[(f * 5 + j) * BS];
+        return v;
+    }
+    __device__ __forceinline__ void st(int f, const Fq52 &v) const
+    {
+#pragma unroll
+        for (int j = 0; j < 5; ++j) s[(f * 5 + j) * BS] = v.l[j];
+    }
+    __device__ __forceinline__ void set(const Xyzz<Fq52> &a) const
+    {
+        st(0, a.x);
+        st(1, a.y);
+        st(2, a.zz);
+        st(3, a.zzz);
+    }
+    __device__ __forceinline__ Xyzz<Fq52> get() const { return {ld(0), ld(1), ld(2), ld(3)}; }
+};
+
+// acc + q (madd-2008-s, the paired form of xyzz_add_affine) on a shared-memory
+// accumulator; q may be infinity
+template <int BS>
+__device__ __forceinline__ void sm_add_affine(const SmXyzz52<BS> &a, const Affine<Fq52> &q)
+{
+    if (q.is_inf()) return;
+    const Fq52 zz = a.ld(2);
+    if (zz.is_zero()) {
+        a.set({q.x, q.y, Fq52::one(), Fq52::one()});
+        return;
+    }
+    Fq52 u2, s2;
+    mul2(q.x, zz, q.y, a.ld(3), u2, s2);
+    const Fq52 p = u2 - a.ld(0);
+    const Fq52 r = s2 - a.ld(1);
+    if (p.is_zero()) {
+        a.set(r.is_zero() ? xyzz_from_affine_dbl(q) : Xyzz<Fq52>::inf());
+        return;
+    }
+    Fq52 pp, rr, ppp, qq, y1ppp, ry, t;
+    mul2(p, p, r, r, pp, rr);
+    mul2(p, pp, a.ld(0), pp, ppp, qq);
+    mul2(a.ld(3), ppp, a.ld(1), ppp, t, y1ppp);
+    a.st(3, t);
+    const Fq52 ox = rr - ppp - dbl(qq);
+    a.st(0, ox);
+    mul2(r, qq - ox, a.ld(2), pp, ry, t);
+    a.st(2, t);
+    a.st(1, ry - y1ppp);
+}
+
+// acc_l1_body for G1 with the accumulator in shared memory (same runs, same
+// flushes, same results)
+template <int BS>
+__device__ __forceinline__ void acc_l1_body_g1s(const uint32_t *__restrict__ offsets,
+                                                const uint32_t *__restrict__ entries,
+                                                const Affine<Fq> *__restrict__ pts, uint32_t nb,
+                                                uint32_t k1, Xyzz<Fq> *__restrict__ partials,
+                                                Xyzz<Fq> *__restrict__ buckets, uint32_t t,
+                                                uint64_t *sm_block)
+{
+    const uint32_t total = offsets[nb];
+    const uint64_t beg64 = uint64_t(t) * k1;
+    if (beg64 >= total) return;
+    const uint32_t beg = uint32_t(beg64);
+    const uint32_t end = min(beg + k1, total);
+    uint32_t b = upper_bound_u32(offsets, nb + 1, beg) - 1; // offsets[b] <= beg < offsets[b + 1]
+    uint32_t bstart = offsets[b], bend = offsets[b + 1];
+    bool first = true;
+    const SmXyzz52<BS> acc{sm_block + threadIdx.x};
+    acc.set(Xyzz<Fq52>::inf());
+    for (uint32_t j = beg; j < end; ++j) {
+        if (j == bend) {
+            if (bstart >= beg)
+                buckets[b] = stx(acc.get());
+            else
+                partials[2ull * t] = stx(acc.get());
+            first = false;
+            acc.set(Xyzz<Fq52>::inf());
+            ++b;
+            int steps = 0;
+            while (offsets[b + 1] <= j && steps < 8) {
+                ++b;
+                ++steps;
+            }
+            if (offsets[b + 1] <= j) b = upper_bound_u32(offsets, nb + 1, j) - 1;
+            bstart = offsets[b];
+            bend = offsets[b + 1];
+        }
+        const uint32_t e = entries[j];
+        Affine<Fq52> p = lda(pts[e & 0x7fffffffu]);
+        if (e >> 31) p = affine_neg(p);
+        sm_add_affine<BS>(acc, p);
+    }
+    if (bstart >= beg && bend <= end)
+        buckets[b] = stx(acc.get());
+    else
+        partials[2ull * t + (first ? 0 : 1)] = stx(acc.get());
+}
+
+// Level 1 kernels.  G1 (FP64 field, paired products passed by value, the
+// accumulator in shared memory) gets a 3-blocks-per-SM register budget: measured
+// against the compiler's own choice (184 registers, 2 blocks) and a 4-block
+// budget (128 registers, more spills), it is the fastest from 2^16 to 2^20
+// points, uniform and sparse.  With the accumulator in registers the same budget
+// spilled 100 B per thread and the kernel took 1.4% longer at 2^20; with it in
+// shared memory a 4-block budget still spills (124 B) and is no faster.  G2
+// keeps the compiler's choice (232 registers, 2 blocks per SM; a 3-block budget
+// spills 284 B per thread and is no faster).
 template <class F>
 __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
                                                  const uint32_t *__restrict__ entries,
@@ -309,15 +423,16 @@ __global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ off
     acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-template <class F>
 __global__ void __launch_bounds__(128, 3) k_acc_l1_g1(const uint32_t *__restrict__ offsets,
                                                        const uint32_t *__restrict__ entries,
-                                                       const Affine<F> *__restrict__ pts,
+                                                       const Affine<Fq> *__restrict__ pts,
                                                        uint32_t nb, uint32_t k1,
-                                                       Xyzz<F> *__restrict__ partials,
-                                                       Xyzz<F> *__restrict__ buckets)
+                                                       Xyzz<Fq> *__restrict__ partials,
+                                                       Xyzz<Fq> *__restrict__ buckets)
 {
-    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x);
+    __shared__ uint64_t sm[20 * 128];
+    acc_l1_body_g1s<128>(offsets, entries, pts, nb, k1, partials, buckets,
+                         blockIdx.x * blockDim.x + threadIdx.x, sm);
 }
 
 // Level 1 of several MSMs of one group in one launch (a batch's MSMs, any sizes):
@@ -331,8 +446,9 @@ struct AccItem {
 };
 static_assert(sizeof(AccItem<Fq>) <= kMsmAccItemBytes, "work-list item size");
 
+// the work-list item of this block (binary search over the items' first blocks)
 template <class F>
-__device__ __forceinline__ void acc_l1_list_body(const AccItem<F> *items, int n_items)
+__device__ __forceinline__ AccItem<F> acc_list_item(const AccItem<F> *items, int n_items)
 {
     int lo = 0, hi = n_items - 1;
     while (lo < hi) {
@@ -342,21 +458,23 @@ __device__ __forceinline__ void acc_l1_list_body(const AccItem<F> *items, int n_
         else
             hi = mid - 1;
     }
-    const AccItem<F> it = items[lo];
-    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
-                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x);
+    return items[lo];
 }
 
 template <class F>
 __global__ void __launch_bounds__(128) k_acc_l1_list(const AccItem<F> *items, int n_items)
 {
-    acc_l1_list_body(items, n_items);
+    const AccItem<F> it = acc_list_item(items, n_items);
+    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
+                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x);
 }
 
-template <class F>
-__global__ void __launch_bounds__(128, 3) k_acc_l1_g1_list(const AccItem<F> *items, int n_items)
+__global__ void __launch_bounds__(128, 3) k_acc_l1_g1_list(const AccItem<Fq> *items, int n_items)
 {
-    acc_l1_list_body(items, n_items);
+    __shared__ uint64_t sm[20 * 128];
+    const AccItem<Fq> it = acc_list_item(items, n_items);
+    acc_l1_body_g1s<128>(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
+                         (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x, sm);
 }
 
 // One group of k2 pieces (spaced `stride` pieces apart) of one bucket; the
@@ -410,7 +528,7 @@ __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ off
 // 256-thread block per SM fits) and a single final block.  Measured fastest for
 // G1 (BS 256) at 2^15, 2^16 and 2^19 buckets and G2 (BS 128) at 2^15 and 2^16.
 // The environment variable NKR_B200_REDUCE_L2 sets it for tuning experiments.
-int first_level_log2(uint32_t m, int log2_bs)
+int first_level_log2(uint32_t m, int log2_bs, int bias)
 {
     static const int forced = [] {
         const char *e = std::getenv("NKR_B200_REDUCE_L2");
@@ -420,7 +538,9 @@ int first_level_log2(uint32_t m, int log2_bs)
     while ((uint64_t(1) << (lg + 1)) <= m) ++lg;
     if (forced >= 0) return forced < lg ? forced : lg;
     const int over = lg - (7 + log2_bs);
-    return over <= 0 ? 0 : over > 4 ? 4 : over;
+    int l2 = (over <= 0 ? 0 : over > 4 ? 4 : over) + bias;
+    l2 = l2 < 0 ? 0 : l2;
+    return l2 < lg ? l2 : lg;
 }
 
 // run += S_b for bucket b: S_b is empty, written whole by the level-1 kernel
@@ -727,7 +847,7 @@ int acc_level1_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, cudaStream_t s
     const uint32_t *offsets = s.offsets.as<uint32_t>();
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[0], st));
     if constexpr (std::is_same<F, Fq>::value)
-        k_acc_l1_g1<F><<<blocks_for(segs, 128), 128, 0, st>>>(
+        k_acc_l1_g1<<<blocks_for(segs, 128), 128, 0, st>>>(
             offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
             a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     else
@@ -764,7 +884,7 @@ int acc_level1_list_t(const MsmAccJob *jobs, int n, void *items_host, void *item
     AccItem<F> *d = static_cast<AccItem<F> *>(items_dev);
     NKR_CUDA(cudaMemcpyAsync(d, items, n * sizeof(AccItem<F>), cudaMemcpyHostToDevice, st));
     if constexpr (std::is_same<F, Fq>::value)
-        k_acc_l1_g1_list<F><<<unsigned(blocks), 128, 0, st>>>(d, n);
+        k_acc_l1_g1_list<<<unsigned(blocks), 128, 0, st>>>(d, n);
     else
         k_acc_l1_list<F><<<unsigned(blocks), 128, 0, st>>>(d, n);
     NKR_CHECK_LAUNCH();
@@ -803,7 +923,7 @@ int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, c
     NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
     // first level: bucket sums (few-piece buckets finished here), L buckets per thread
-    const int log2_l = first_level_log2(m, kLog2BS);
+    const int log2_l = first_level_log2(m, kLog2BS, a.first_level_bias);
     const uint32_t L = 1u << log2_l;
     const uint64_t items = uint64_t(sets) * m;
     k_reduce_first<F><<<blocks_for(items / L, 128), 128, 0, st>>>(
@@ -846,7 +966,7 @@ int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     // first reduction level output: one item per L buckets (L as in acc_run_t)
     constexpr int kLog2BS = sizeof(F) == sizeof(Fq) ? 8 : 7; // block size of acc_run_t's levels
-    const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B, kLog2BS)) + 1;
+    const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B, kLog2BS, a.first_level_bias)) + 1;
     NKR_TRY(a.partials.alloc(2 * std::max<uint64_t>(sh.segments_max(), 1) * sizeof(Xyzz<F>),
                              "msm partial sums"));
     NKR_TRY(a.buckets.alloc(uint64_t(sh.nb) * sizeof(Xyzz<F>), "msm buckets"));

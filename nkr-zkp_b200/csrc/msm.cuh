@@ -85,6 +85,9 @@ struct MsmAcc {
     // level, after the last reduction level and the final combination
     bool timing = false;
     cudaEvent_t ev_acc[5] = {};
+    // added to the first reduction level's log2 buckets per thread (set before
+    // msm_acc_alloc): larger levels do less work in more dependent steps
+    int first_level_bias = 0;
     size_t device_bytes() const
     {
         return partials.bytes + buckets.bytes + lead_off.bytes + red_a.bytes + red_r.bytes +
