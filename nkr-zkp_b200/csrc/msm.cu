@@ -56,6 +56,20 @@ __device__ __forceinline__ void for_each_digit(const Fr &s, int c, int W, Fn &&f
     }
 }
 
+// Lanes of this warp whose scalar equals this lane's (all eight words): equal
+// scalars have equal digits, so one lane per group updates the bucket counters
+// for the whole group.  Matching once per scalar replaces a match per digit
+// (repeated scalars are what makes buckets hot in sparse witnesses; distinct
+// uniform scalars form groups of one).
+__device__ __forceinline__ unsigned equal_scalar_lanes(unsigned mask, const Fr &s)
+{
+    unsigned peers = mask;
+#pragma unroll
+    for (int w = 0; w < 8; w += 2)
+        peers &= __match_any_sync(mask, uint64_t(s.v[w]) | (uint64_t(s.v[w + 1]) << 32));
+    return peers;
+}
+
 __global__ void k_digits_count(const Fr *__restrict__ scalars, const uint32_t *__restrict__ gather,
                                uint64_t n, int c, int W, bool folded, uint32_t B,
                                Fr *__restrict__ canon, uint32_t *__restrict__ counts)
@@ -68,14 +82,13 @@ __global__ void k_digits_count(const Fr *__restrict__ scalars, const uint32_t *_
         canon[i] = s;
     }
     const int lane = threadIdx.x & 31;
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!live) return;
+    const unsigned peers = equal_scalar_lanes(act, s);
+    if (lane != __ffs(peers) - 1) return;
+    const uint32_t group = uint32_t(__popc(peers));
     for_each_digit(s, c, W, [&](int k, bool has, uint32_t b, bool) {
-        has = has && live;
-        const unsigned act = __ballot_sync(0xffffffffu, has);
-        if (has) {
-            const uint32_t bucket = (folded ? 0u : uint32_t(k) * B) + b;
-            const unsigned peers = __match_any_sync(act, bucket);
-            if (lane == __ffs(peers) - 1) atomicAdd(&counts[bucket], uint32_t(__popc(peers)));
-        }
+        if (has) atomicAdd(&counts[(folded ? 0u : uint32_t(k) * B) + b], group);
     });
 }
 
@@ -84,19 +97,21 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = i < n;
-    const Fr s = live ? canon[i] : Fr::zero();
     const int lane = threadIdx.x & 31;
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!live) return;
+    const Fr s = canon[i];
+    const unsigned peers = equal_scalar_lanes(act, s);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t group = uint32_t(__popc(peers));
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
     for_each_digit(s, c, W, [&](int k, bool has, uint32_t b, bool negd) {
-        has = has && live;
-        const unsigned act = __ballot_sync(0xffffffffu, has);
+        // the group's lanes agree on every digit, so they take this branch together
         if (has) {
             const uint32_t bucket = (folded ? 0u : uint32_t(k) * B) + b;
-            const unsigned peers = __match_any_sync(act, bucket);
-            const int leader = __ffs(peers) - 1;
             uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(&cursor[bucket], uint32_t(__popc(peers)));
+            if (lane == leader) base = atomicAdd(&cursor[bucket], group);
             base = __shfl_sync(peers, base, leader);
-            const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
             const uint32_t point = folded ? uint32_t(uint64_t(k) * n + i) : uint32_t(i);
             entries[base + rank] = point | (negd ? 0x80000000u : 0u);
         }
