@@ -405,6 +405,7 @@ static int msm_plain(nkr_b200_ctx *ctx, int group, const void *bases, const void
     MsmBases b;
     NKR_TRY(msm_bases_build(b, group, bases, false, n, false, 0, false, st));
     MsmScratch s;
+    s.acc.lane_pairs = true; // an MSM alone: latency-bound reduction levels
     NKR_TRY(msm_scratch_alloc(s, group, b.shape));
     DevBuf ds;
     NKR_TRY(ds.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
@@ -443,6 +444,7 @@ int nkr_b200_msm_bases_create(nkr_b200_ctx *ctx, int group, const void *bases, u
     NKR_TRY(msm_scratch_alloc(h->scratch, group, h->bases.shape));
     for (auto &e : h->scratch.acc.ev_acc) NKR_CUDA(cudaEventCreate(&e));
     h->scratch.acc.timing = true;
+    h->scratch.acc.lane_pairs = true; // MSMs alone: latency-bound reduction levels
     NKR_TRY(h->scalars.alloc(std::max<uint64_t>(n, 1) * 32, "msm scalars"));
     *out = h.release();
     return NKR_B200_OK;

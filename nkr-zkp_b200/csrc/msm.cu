@@ -15,6 +15,78 @@
 
 namespace nkr {
 
+// --------------------------------------------------------------------------
+// lane pairs.  The bucket reduction levels are chains of dependent additions
+// run by few threads, so there each addition is computed by two lanes: the
+// curve formulas issue their products in independent pairs (mul2), and a lane
+// pair computes one product of each pair and exchanges the results.  Everything
+// else is computed by both lanes alike, so a pair stays converged.
+// --------------------------------------------------------------------------
+template <class B>
+struct Pair2 : B {
+    using base = B;
+    Pair2() = default;
+    __device__ __forceinline__ Pair2(const B &b) : B(b) {}
+    __device__ __forceinline__ static Pair2 zero() { return B::zero(); }
+    __device__ __forceinline__ static Pair2 one() { return B::one(); }
+};
+template <class B>
+__device__ __forceinline__ Pair2<B> operator+(const Pair2<B> &a, const Pair2<B> &b)
+{
+    return static_cast<const B &>(a) + static_cast<const B &>(b);
+}
+template <class B>
+__device__ __forceinline__ Pair2<B> operator-(const Pair2<B> &a, const Pair2<B> &b)
+{
+    return static_cast<const B &>(a) - static_cast<const B &>(b);
+}
+template <class B>
+__device__ __forceinline__ Pair2<B> operator*(const Pair2<B> &a, const Pair2<B> &b)
+{
+    return static_cast<const B &>(a) * static_cast<const B &>(b);
+}
+template <class B>
+__device__ __forceinline__ Pair2<B> dbl(const Pair2<B> &a) { return dbl(static_cast<const B &>(a)); }
+template <class B>
+__device__ __forceinline__ Pair2<B> sqr(const Pair2<B> &a) { return sqr(static_cast<const B &>(a)); }
+
+__device__ __forceinline__ Fq52 shfl_xor1(unsigned mask, const Fq52 &a)
+{
+    Fq52 r;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) r.l[j] = __shfl_xor_sync(mask, a.l[j], 1);
+    return r;
+}
+__device__ __forceinline__ Fq2 shfl_xor1(unsigned mask, const Fq2 &a)
+{
+    Fq2 r;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        r.c0.v[j] = __shfl_xor_sync(mask, a.c0.v[j], 1);
+        r.c1.v[j] = __shfl_xor_sync(mask, a.c1.v[j], 1);
+    }
+    return r;
+}
+
+// the pair of lanes (2j, 2j + 1) of the calling lane
+__device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31u) & 30u); }
+
+// x = a b, y = c d: the even lane computes a b, the odd lane c d
+template <class B>
+__device__ __forceinline__ void mul2(const Pair2<B> &a, const Pair2<B> &b, const Pair2<B> &c,
+                                     const Pair2<B> &d, Pair2<B> &x, Pair2<B> &y)
+{
+    const bool odd = threadIdx.x & 1u;
+    const B m = static_cast<const B &>(odd ? c : a) * static_cast<const B &>(odd ? d : b);
+    const B o = shfl_xor1(pair_mask(), m);
+    x = odd ? o : m;
+    y = odd ? m : o;
+}
+template <class B>
+struct HasPairedMul<Pair2<B>> {
+    static constexpr bool value = true;
+};
+
 namespace {
 
 // --------------------------------------------------------------------------
@@ -148,19 +220,42 @@ struct MsmArith<Fq2> {
 template <class F>
 using CF = typename MsmArith<F>::type;
 
-// Compute type of the bucket reduction levels (first level, block levels, final
-// combination): latency-bound chains of dependent additions, where G2 gains from
-// the lazily reduced Fq2 product (Fq2L, field.cuh).
+// Compute type and shape of the bucket reduction levels (first level, block
+// levels, final combination): latency-bound chains of dependent additions, with
+// LANES lanes per item.  G2 computes in the lazily reduced Fq2 product (Fq2L,
+// field.cuh), 128 items per block; an MSM alone (MsmAcc::lane_pairs) runs it on
+// lane pairs (Pair2): at 2^18 points the block levels 1.21 -> 0.85 ms and the
+// first level 0.36 -> 0.28 ms.  Inside a prove the G2 levels overlap the other
+// MSMs' level-1 kernels, and there the pairs' 256-thread blocks, which take a
+// whole SM's registers, cost more than they save (2^20 prove 19.09 vs 18.97 ms),
+// so a prove keeps one lane per item.  G1 keeps one lane per item and 256 items
+// per block: on lane pairs (128 items per block, the register budget of a
+// 256-thread block) its block levels are shorter but its first level takes
+// twice the buckets per pair (2^20 MSM 4.31 vs 4.25 ms; a 2^20 prove 19.16 ms).
 template <class F>
-struct MsmReduceArith {
+struct ReduceBase {
     using type = CF<F>;
 };
 template <>
-struct MsmReduceArith<Fq2> {
+struct ReduceBase<Fq2> {
     using type = Fq2L;
 };
-template <class F>
-using CR = typename MsmReduceArith<F>::type;
+template <class F, int LANES>
+struct MsmReduceArith {
+    using type = typename std::conditional<LANES == 2, Pair2<typename ReduceBase<F>::type>,
+                                           typename ReduceBase<F>::type>::type;
+    static constexpr int lanes = LANES;
+    static constexpr int items = (LANES == 1 && sizeof(F) == sizeof(Fq)) ? 256 : 128;
+    static constexpr int log2_items = items == 256 ? 8 : 7;
+};
+template <class C>
+struct BaseOf {
+    using type = C;
+};
+template <class B>
+struct BaseOf<Pair2<B>> {
+    using type = B;
+};
 
 __device__ __forceinline__ Fq52 msm_in(const Fq &x) { return to52(x); }
 __device__ __forceinline__ Fq msm_out(const Fq52 &x) { return from52(x); }
@@ -177,10 +272,11 @@ __device__ __forceinline__ Xyzz<CF<F>> ldx(const Xyzz<F> &s)
     return {msm_in(s.x), msm_in(s.y), msm_in(s.zz), msm_in(s.zzz)};
 }
 
-template <class F>
-__device__ __forceinline__ Xyzz<CR<F>> ldr(const Xyzz<F> &s)
+template <class C, class F>
+__device__ __forceinline__ Xyzz<C> ldr(const Xyzz<F> &s)
 {
-    return {msm_in(s.x), msm_in(s.y), msm_in(s.zz), msm_in(s.zzz)};
+    using B = typename BaseOf<C>::type;
+    return {B(msm_in(s.x)), B(msm_in(s.y)), B(msm_in(s.zz)), B(msm_in(s.zzz))};
 }
 
 template <class C>
@@ -537,11 +633,12 @@ __global__ void __launch_bounds__(128) k_acc_up(const uint32_t *__restrict__ off
 // bucket reduction: sum_b b * S_b per set, then + sum_b S_b
 // --------------------------------------------------------------------------
 
-// Buckets per thread of the first reduction level (log2).  The block levels
-// that follow are latency bound (dependent additions), so the first level leaves
-// about 128 x BS items: the next level is then one wave of 128 blocks (at most one
-// 256-thread block per SM fits) and a single final block.  Measured fastest for
-// G1 (BS 256) at 2^15, 2^16 and 2^19 buckets and G2 (BS 128) at 2^15 and 2^16.
+// Buckets per thread (G2: per lane pair) of the first reduction level (log2).
+// The block levels that follow are latency bound (dependent additions), so the
+// first level leaves about 128 x BS items: the next level is then one wave of 128
+// blocks (at most one 256-thread block per SM fits) and a single final block.
+// Measured fastest for G1 (BS 256) at 2^15, 2^16 and 2^19 buckets and G2 (BS 128)
+// at 2^15 and 2^16.
 // The environment variable NKR_B200_REDUCE_L2 sets it for tuning experiments.
 int first_level_log2(uint32_t m, int log2_bs, int bias)
 {
@@ -561,8 +658,8 @@ int first_level_log2(uint32_t m, int log2_bs, int bias)
 // run += S_b for bucket b: S_b is empty, written whole by the level-1 kernel
 // (one piece) or by the fix-up levels (more than kSmallPieces pieces), or else
 // its few pieces are added straight from the partial slots.
-template <class F>
-__device__ __forceinline__ Xyzz<CR<F>> add_bucket_sum(Xyzz<CR<F>> run,
+template <class C, class F>
+__device__ __forceinline__ Xyzz<C> add_bucket_sum(Xyzz<C> run,
                                                       const uint32_t *__restrict__ offsets,
                                                       const Xyzz<F> *__restrict__ partials,
                                                       const Xyzz<F> *__restrict__ buckets, uint32_t b,
@@ -571,16 +668,16 @@ __device__ __forceinline__ Xyzz<CR<F>> add_bucket_sum(Xyzz<CR<F>> run,
     const uint32_t lo = offsets[b], hi = offsets[b + 1];
     if (hi == lo) return run;
     const Pieces pc{lo / k1, (hi - 1) / k1 - lo / k1 + 1};
-    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldr(buckets[b]));
-    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldr(partials[pc.slot(lo, k1, k)]));
+    if (pc.count == 1 || pc.count > kSmallPieces) return xyzz_add(run, ldr<C>(buckets[b]));
+    for (uint32_t k = 0; k < pc.count; ++k) run = xyzz_add(run, ldr<C>(partials[pc.slot(lo, k1, k)]));
     return run;
 }
 
-// Work-efficient first reduction level: a thread takes L consecutive buckets
+// Work-efficient first reduction level: a thread (G2: a lane pair) takes L consecutive buckets
 // and forms T = sum_i i S_i and R = sum_i S_i by running sums (2 additions per
 // bucket), emitting one (A = T, R) item per L buckets with unit L for the block
 // levels that follow.  Bucket sums of few pieces are finished here.
-template <class F>
+template <class F, int LANES>
 __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict__ offsets,
                                                        const Xyzz<F> *__restrict__ partials,
                                                        const Xyzz<F> *__restrict__ buckets,
@@ -588,14 +685,16 @@ __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict
                                                        Xyzz<F> *__restrict__ a_out,
                                                        Xyzz<F> *__restrict__ r_out)
 {
-    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    using C = typename MsmReduceArith<F, LANES>::type;
+    const uint64_t t = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / LANES; // the lanes' item
     if (t * L >= items) return;
     const uint64_t base = t * L;
-    Xyzz<CR<F>> run = Xyzz<CR<F>>::inf(), tri = Xyzz<CR<F>>::inf();
+    Xyzz<C> run = Xyzz<C>::inf(), tri = Xyzz<C>::inf();
     for (int i = int(L) - 1; i >= 0; --i) {
-        run = add_bucket_sum(run, offsets, partials, buckets, uint32_t(base + i), k1);
+        run = add_bucket_sum<C>(run, offsets, partials, buckets, uint32_t(base + i), k1);
         if (i > 0) tri = xyzz_add(tri, run);
     }
+    if (threadIdx.x % LANES) return;
     a_out[t] = stx(tri);
     r_out[t] = stx(run);
 }
@@ -607,33 +706,35 @@ __global__ void __launch_bounds__(128) k_reduce_first(const uint32_t *__restrict
 // with a Hillis-Steele scan in shared memory (log2 BS dependent additions),
 // then sum_c c R_c = sum_{c >= 1} Suf_c and sum_c A_c by two tree sums on
 // disjoint threads, so a level costs about 2 log2(BS) dependent additions
-// instead of 2 BS.
+// instead of 2 BS.  With lane pairs (G2) item c belongs to lanes (2c, 2c + 1)
+// and the even lane stores.
 // Output per block: A' = sum A_c + U sum_c c R_c, R' = sum R_c.
-template <class F, int BS>
-__global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__ a_in,
+template <class F, int BS, int LANES>
+__global__ void __launch_bounds__(BS * LANES) k_reduce_block(const Xyzz<F> *__restrict__ a_in,
                                                       const Xyzz<F> *__restrict__ r_in,
                                                       uint32_t m, int log2_unit,
                                                       Xyzz<F> *__restrict__ a_out,
                                                       Xyzz<F> *__restrict__ r_out)
 {
-    using C = CR<F>;
+    using C = typename MsmReduceArith<F, LANES>::type;
     extern __shared__ uint8_t smem_raw[];
     Xyzz<C> *buf0 = reinterpret_cast<Xyzz<C> *>(smem_raw);
     Xyzz<C> *buf1 = buf0 + BS;
     const uint32_t blocks_per_set = (m + BS - 1) / BS;
     const uint32_t set = blockIdx.x / blocks_per_set;
     const uint32_t blk = blockIdx.x % blocks_per_set;
-    const int i = threadIdx.x;
+    const int i = threadIdx.x / LANES;
+    const bool lead = threadIdx.x % LANES == 0;
     const uint64_t idx = uint64_t(blk) * BS + i;
     const bool live = idx < m;
     const uint64_t g = uint64_t(set) * m + idx;
-    Xyzz<C> v = live ? ldr(r_in[g]) : Xyzz<C>::inf();
-    buf0[i] = v;
+    Xyzz<C> v = live ? ldr<C>(r_in[g]) : Xyzz<C>::inf();
+    if (lead) buf0[i] = v;
     __syncthreads();
     Xyzz<C> *cur = buf0, *nxt = buf1;
     for (int d = 1; d < BS; d <<= 1) {
         if (i + d < BS) v = xyzz_add(v, cur[i + d]);
-        nxt[i] = v;
+        if (lead) nxt[i] = v;
         __syncthreads();
         Xyzz<C> *t = cur;
         cur = nxt;
@@ -642,36 +743,45 @@ __global__ void __launch_bounds__(BS) k_reduce_block(const Xyzz<F> *__restrict__
     // v = Suf_i.  R' = Suf_0; weighted part = sum_{i >= 1} Suf_i; A part = sum A_i
     const Xyzz<C> total = cur[0];
     __syncthreads();
-    buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
-    buf1[i] = (a_in && live) ? ldr(a_in[g]) : Xyzz<C>::inf();
+    if (lead) {
+        buf0[i] = i >= 1 ? v : Xyzz<C>::inf();
+        buf1[i] = (a_in && live) ? ldr<C>(a_in[g]) : Xyzz<C>::inf();
+    }
     __syncthreads();
-    // the two tree sums run side by side on disjoint threads (first s: weighted
-    // suffix sums, next s: A items), one addition per thread and step
+    // the two tree sums run side by side on disjoint lane pairs (first s: weighted
+    // suffix sums, next s: A items), one addition per pair and step; the pair has
+    // read its operands before the even lane overwrites the first (__syncwarp)
     for (int s = BS / 2; s > 0; s >>= 1) {
         if (i < s) {
-            buf0[i] = xyzz_add(buf0[i], buf0[i + s]);
+            const Xyzz<C> r = xyzz_add(buf0[i], buf0[i + s]);
+            if constexpr (LANES == 2) __syncwarp(pair_mask());
+            if (lead) buf0[i] = r;
         } else if (i < 2 * s) {
             const int j = i - s;
-            buf1[j] = xyzz_add(buf1[j], buf1[j + s]);
+            const Xyzz<C> r = xyzz_add(buf1[j], buf1[j + s]);
+            if constexpr (LANES == 2) __syncwarp(pair_mask());
+            if (lead) buf1[j] = r;
         }
         __syncthreads();
     }
     if (i == 0) {
         Xyzz<C> w = buf0[0];
         for (int d = 0; d < log2_unit; ++d) w = xyzz_dbl(w);
-        const uint32_t o = set * blocks_per_set + blk;
-        a_out[o] = stx(xyzz_add(w, buf1[0]));
-        r_out[o] = stx(total);
+        const Xyzz<C> a = xyzz_add(w, buf1[0]);
+        if (lead) {
+            const uint32_t o = set * blocks_per_set + blk;
+            a_out[o] = stx(a);
+            r_out[o] = stx(total);
+        }
     }
 }
 
 // XYZZ -> libff Jacobian layout without inversion: with Z = ZZ ZZZ,
 // X' = X ZZ ZZZ^2 and Y' = Y ZZ^3 ZZZ^2 represent the same affine point; the
 // coordinates leave the R' domain here (back to the library's R = 2^256).
-template <class F>
-__device__ __forceinline__ void store_jacobian(const Xyzz<CR<F>> &p, F *out)
+template <class C, class F>
+__device__ __forceinline__ void store_jacobian(const Xyzz<C> &p, F *out)
 {
-    using C = CR<F>;
     if (p.is_inf()) {
         out[0] = F::zero();
         out[1] = F::one();
@@ -685,18 +795,19 @@ __device__ __forceinline__ void store_jacobian(const Xyzz<CR<F>> &p, F *out)
     out[2] = msm_out(msm_leave(p.zz * p.zzz));
 }
 
-template <class F>
+// one thread (G2: the lane pair 0, 1); lane 0 stores
+template <class F, int LANES>
 __global__ void k_finalize(const Xyzz<F> *a, const Xyzz<F> *r, int sets, int c, F *out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    using C = CR<F>;
+    if (threadIdx.x >= unsigned(LANES) || blockIdx.x != 0) return;
+    using C = typename MsmReduceArith<F, LANES>::type;
     Xyzz<C> acc = Xyzz<C>::inf();
     for (int k = sets - 1; k >= 0; --k) {
         if (k != sets - 1)
             for (int d = 0; d < c; ++d) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, a ? xyzz_add(ldr(a[k]), ldr(r[k])) : ldr(r[k]));
+        acc = xyzz_add(acc, a ? xyzz_add(ldr<C>(a[k]), ldr<C>(r[k])) : ldr<C>(r[k]));
     }
-    store_jacobian<F>(acc, out);
+    if (threadIdx.x == 0) store_jacobian(acc, out);
 }
 
 // Resident bases enter the R' domain once they are final (x 2^4 mod p per
@@ -906,6 +1017,54 @@ int acc_level1_list_t(const MsmAccJob *jobs, int n, void *items_host, void *item
     return NKR_B200_OK;
 }
 
+// The reduction levels of an MSM whose buckets are final: first level, block
+// levels, final combination, with LANES lanes per item.
+template <class F, int LANES>
+int reduce_run(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    using RA = MsmReduceArith<F, LANES>;
+    const MsmShape &sh = bs.shape;
+    const uint32_t *offsets = s.offsets.as<uint32_t>();
+    const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
+    uint32_t m = sh.B;
+    Xyzz<F> *bufs_a[2] = {a.red_a.as<Xyzz<F>>(), a.red_a2.as<Xyzz<F>>()};
+    Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
+    constexpr int BS = RA::items;
+    constexpr int kLog2BS = RA::log2_items;
+    const size_t smem = 2 * BS * sizeof(Xyzz<typename RA::type>);
+    NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS, LANES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)));
+    // first level: bucket sums (few-piece buckets finished here), L buckets per item
+    const int log2_l = first_level_log2(m, kLog2BS, a.first_level_bias);
+    const uint32_t L = 1u << log2_l;
+    const uint64_t items = uint64_t(sets) * m;
+    k_reduce_first<F, LANES><<<blocks_for(LANES * (items / L), 128), 128, 0, st>>>(
+        offsets, a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), items, L, uint32_t(sh.k1), bufs_a[0],
+        bufs_r[0]);
+    NKR_CHECK_LAUNCH();
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[3], st));
+    const Xyzz<F> *a_in = bufs_a[0];
+    const Xyzz<F> *r_in = bufs_r[0];
+    int flip = 1;
+    m /= L;
+    int log2_unit = log2_l;
+    while (m > 1) {
+        const uint32_t per_set = (m + BS - 1) / BS;
+        k_reduce_block<F, BS, LANES><<<sets * per_set, LANES * BS, smem, st>>>(
+            a_in, r_in, m, log2_unit, bufs_a[flip], bufs_r[flip]);
+        NKR_CHECK_LAUNCH();
+        a_in = bufs_a[flip];
+        r_in = bufs_r[flip];
+        flip ^= 1;
+        m = per_set;
+        log2_unit += kLog2BS;
+    }
+    k_finalize<F, LANES><<<1, 32, 0, st>>>(a_in, r_in, int(sets), sh.c, static_cast<F *>(out_dev));
+    NKR_CHECK_LAUNCH();
+    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[4], st));
+    return NKR_B200_OK;
+}
+
 template <class F>
 int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
 {
@@ -927,45 +1086,10 @@ int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, c
         NKR_CHECK_LAUNCH();
     }
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[2], st));
-    // bucket reduction levels
-    const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
-    uint32_t m = sh.B;
-    Xyzz<F> *bufs_a[2] = {a.red_a.as<Xyzz<F>>(), a.red_a2.as<Xyzz<F>>()};
-    Xyzz<F> *bufs_r[2] = {a.red_r.as<Xyzz<F>>(), a.red_r2.as<Xyzz<F>>()};
-    constexpr int BS = sizeof(F) == sizeof(Fq) ? 256 : 128; // G1: 256 buckets per block, G2: 128
-    constexpr int kLog2BS = BS == 256 ? 8 : 7;
-    const size_t smem = 2 * BS * sizeof(Xyzz<CR<F>>);
-    NKR_CUDA(cudaFuncSetAttribute(k_reduce_block<F, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem)));
-    // first level: bucket sums (few-piece buckets finished here), L buckets per thread
-    const int log2_l = first_level_log2(m, kLog2BS, a.first_level_bias);
-    const uint32_t L = 1u << log2_l;
-    const uint64_t items = uint64_t(sets) * m;
-    k_reduce_first<F><<<blocks_for(items / L, 128), 128, 0, st>>>(
-        offsets, a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), items, L, uint32_t(sh.k1), bufs_a[0],
-        bufs_r[0]);
-    NKR_CHECK_LAUNCH();
-    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[3], st));
-    const Xyzz<F> *a_in = bufs_a[0];
-    const Xyzz<F> *r_in = bufs_r[0];
-    int flip = 1;
-    m /= L;
-    int log2_unit = log2_l;
-    while (m > 1) {
-        const uint32_t per_set = (m + BS - 1) / BS;
-        k_reduce_block<F, BS><<<sets * per_set, BS, smem, st>>>(a_in, r_in, m, log2_unit, bufs_a[flip],
-                                                               bufs_r[flip]);
-        NKR_CHECK_LAUNCH();
-        a_in = bufs_a[flip];
-        r_in = bufs_r[flip];
-        flip ^= 1;
-        m = per_set;
-        log2_unit += kLog2BS;
-    }
-    k_finalize<F><<<1, 32, 0, st>>>(a_in, r_in, int(sets), sh.c, static_cast<F *>(out_dev));
-    NKR_CHECK_LAUNCH();
-    if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[4], st));
-    return NKR_B200_OK;
+    // bucket reduction levels (G2 alone: on lane pairs)
+    if constexpr (std::is_same<F, Fq2>::value)
+        if (a.lane_pairs) return reduce_run<F, 2>(bs, s, a, out_dev, st);
+    return reduce_run<F, 1>(bs, s, a, out_dev, st);
 }
 
 template <class F>
@@ -980,7 +1104,10 @@ int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
 {
     const uint32_t sets = sh.folded ? 1u : uint32_t(sh.W);
     // first reduction level output: one item per L buckets (L as in acc_run_t)
-    constexpr int kLog2BS = sizeof(F) == sizeof(Fq) ? 8 : 7; // block size of acc_run_t's levels
+    // items per block of the reduction levels (the same for one and two lanes per item)
+    constexpr int kLog2BS = MsmReduceArith<F, 1>::log2_items;
+    static_assert(MsmReduceArith<F, 1>::log2_items == MsmReduceArith<F, 2>::log2_items || sizeof(F) == sizeof(Fq),
+                  "G2 reduction buffers are sized for one block shape");
     const uint64_t red = uint64_t(sets) * (sh.B >> first_level_log2(sh.B, kLog2BS, a.first_level_bias)) + 1;
     NKR_TRY(a.partials.alloc(2 * std::max<uint64_t>(sh.segments_max(), 1) * sizeof(Xyzz<F>),
                              "msm partial sums"));

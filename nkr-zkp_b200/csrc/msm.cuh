@@ -88,6 +88,9 @@ struct MsmAcc {
     // added to the first reduction level's log2 buckets per thread (set before
     // msm_acc_alloc): larger levels do less work in more dependent steps
     int first_level_bias = 0;
+    // G2 reduction levels on lane pairs (two lanes per item): shorter for an MSM
+    // alone, but inside a prove the wider blocks crowd out the other MSMs' work
+    bool lane_pairs = false;
     size_t device_bytes() const
     {
         return partials.bytes + buckets.bytes + lead_off.bytes + red_a.bytes + red_r.bytes +
