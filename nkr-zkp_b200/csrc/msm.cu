@@ -196,7 +196,9 @@ __global__ void k_scatter(const Fr *__restrict__ canon, uint64_t n, int c, int W
 // values in the 8 x 32-bit layout of Fq, converted at entry (bases) and exit
 // (result).  G2 arithmetic stays on the integer pipe (Fq2, R = 2^256): measured,
 // its FP64 form (Fq2 products as three interleaved 52-bit products) needs all 255
-// registers and ran 34% slower at 2^18 points.  The same holds for the G2
+// registers and ran 34% slower at 2^18 points; with the accumulator in shared
+// memory as for G1 (254 registers, bases in R' from prepare, flushes leaving R')
+// the level-1 kernel took 7.96 instead of 3.48 ms.  The same holds for the G2
 // reduction levels alone, although they are latency bound (a 32-bit product is
 // one long carry chain): in the FP64 form they spill 600 B per thread and took
 // 1.81 instead of 1.53 ms at 2^18; with the three Karatsuba products of an Fq2
@@ -1209,6 +1211,7 @@ int msm_bases_build(MsmBases &b, int group, const void *jac, bool jac_on_device,
         k_bases_to_r260<Fq><<<blocks_for(total, 128), 128, 0, st>>>(b.pts.as<G1Affine>(), total);
         NKR_CHECK_LAUNCH();
     }
+
     NKR_CUDA(cudaStreamSynchronize(st));
     return NKR_B200_OK;
 }
