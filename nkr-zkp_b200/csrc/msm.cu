@@ -352,69 +352,20 @@ struct LoadLeaders {
     }
 };
 
-// Level 1: thread t sums the fixed segment [t K1, (t+1) K1) of the sorted
-// entries, split into runs at bucket boundaries, so every lane of a warp does
-// the same number of mixed additions whatever the bucket sizes.  A run that is
-// a whole bucket is written to the bucket; the segment's first / last run, when
-// its bucket continues outside the segment, goes to partial slot 2t / 2t + 1.
-template <class F>
-__device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets,
-                                            const uint32_t *__restrict__ entries,
-                                            const Affine<F> *__restrict__ pts, uint32_t nb,
-                                            uint32_t k1, Xyzz<F> *__restrict__ partials,
-                                            Xyzz<F> *__restrict__ buckets, uint32_t t)
-{
-    const uint32_t total = offsets[nb];
-    const uint64_t beg64 = uint64_t(t) * k1;
-    if (beg64 >= total) return;
-    const uint32_t beg = uint32_t(beg64);
-    const uint32_t end = min(beg + k1, total);
-    uint32_t b = upper_bound_u32(offsets, nb + 1, beg) - 1; // offsets[b] <= beg < offsets[b + 1]
-    uint32_t bstart = offsets[b], bend = offsets[b + 1];
-    bool first = true;
-    using C = CF<F>;
-    Xyzz<C> acc = Xyzz<C>::inf();
-    // one flat loop with the same trip count in every lane keeps the additions
-    // converged; the flush at a bucket boundary is a short divergent branch
-    for (uint32_t j = beg; j < end; ++j) {
-        if (j == bend) {
-            if (bstart >= beg)
-                buckets[b] = stx(acc); // the bucket started and ended inside the segment
-            else
-                partials[2ull * t] = stx(acc); // first run, bucket began in an earlier segment
-            first = false;
-            acc = Xyzz<C>::inf();
-            // next nonempty bucket: usually adjacent, else search
-            ++b;
-            int steps = 0;
-            while (offsets[b + 1] <= j && steps < 8) {
-                ++b;
-                ++steps;
-            }
-            if (offsets[b + 1] <= j) b = upper_bound_u32(offsets, nb + 1, j) - 1;
-            bstart = offsets[b];
-            bend = offsets[b + 1];
-        }
-        const uint32_t e = entries[j];
-        Affine<C> p = lda(pts[e & 0x7fffffffu]);
-        if (e >> 31) p = affine_neg(p);
-        acc = xyzz_add_affine(acc, p);
-    }
-    if (bstart >= beg && bend <= end)
-        buckets[b] = stx(acc);
-    else
-        partials[2ull * t + (first ? 0 : 1)] = stx(acc);
-}
-
-// G1 level 1 with the accumulator in shared memory.  Across the out-of-line
-// product calls of a mixed addition the four accumulator coordinates were live
-// in registers (40 of the 168 the 3-blocks-per-SM budget allows); kept in
-// shared memory and loaded where a product needs them, they leave registers
-// for a 4-blocks-per-SM budget.  Layout: structure of arrays, word w of thread
-// i at w * BS + i, so a warp's 64-bit accesses are conflict-free.
+// Level-1 accumulators live in shared memory.  Across the out-of-line product
+// calls of a mixed addition the four accumulator coordinates were live in
+// registers (G1: 40 of the 168 the 3-blocks-per-SM budget allows, with 100 B of
+// spills per thread; G2: 64 of 232, 2 blocks per SM); kept in shared memory and
+// loaded where a product needs them, G1 runs its 3-block budget without spills
+// (1.4% faster at 2^20) and G2 fits 3 blocks per SM in 167 registers without
+// spills (6% faster at 2^18).  Layout: structure of arrays, word w of thread i
+// at w * BS + i, so a warp's accesses are conflict-free.
+//
+// G1: Fq52 coordinates (5 x 64-bit words), R' domain throughout.
 template <int BS>
 struct SmXyzz52 {
-    uint64_t *s; // the block's area + threadIdx.x
+    using point = Affine<Fq52>;
+    uint64_t *s; // the block's area + threadIdx.x; 20 words per thread
     __device__ __forceinline__ Fq52 ld(int f) const
     {
         Fq52 v;
@@ -434,50 +385,118 @@ struct SmXyzz52 {
         st(2, a.zz);
         st(3, a.zzz);
     }
-    __device__ __forceinline__ Xyzz<Fq52> get() const { return {ld(0), ld(1), ld(2), ld(3)}; }
+    __device__ __forceinline__ Xyzz<Fq> out() const { return stx(Xyzz<Fq52>{ld(0), ld(1), ld(2), ld(3)}); }
+    __device__ __forceinline__ static point load(const Affine<Fq> &p) { return lda(p); }
 };
 
-// acc + q (madd-2008-s, the paired form of xyzz_add_affine) on a shared-memory
-// accumulator; q may be infinity
+// G2: Fq2 coordinates (16 x 32-bit words), the library's Montgomery domain.
 template <int BS>
-__device__ __forceinline__ void sm_add_affine(const SmXyzz52<BS> &a, const Affine<Fq52> &q)
+struct SmXyzzFq2 {
+    using point = Affine<Fq2>;
+    uint32_t *s; // the block's area + threadIdx.x; 64 words per thread
+    __device__ __forceinline__ Fq2 ld(int f) const
+    {
+        Fq2 v;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            v.c0.v[j] = s[(f * 16 + j) * BS];
+            v.c1.v[j] = s[(f * 16 + 8 + j) * BS];
+        }
+        return v;
+    }
+    __device__ __forceinline__ void st(int f, const Fq2 &v) const
+    {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            s[(f * 16 + j) * BS] = v.c0.v[j];
+            s[(f * 16 + 8 + j) * BS] = v.c1.v[j];
+        }
+    }
+    __device__ __forceinline__ void set(const Xyzz<Fq2> &a) const
+    {
+        st(0, a.x);
+        st(1, a.y);
+        st(2, a.zz);
+        st(3, a.zzz);
+    }
+    __device__ __forceinline__ Xyzz<Fq2> out() const { return {ld(0), ld(1), ld(2), ld(3)}; }
+    __device__ __forceinline__ static point load(const Affine<Fq2> &p) { return p; }
+};
+
+// acc + q (madd-2008-s: 8M + 2S) on a shared-memory accumulator, q may be
+// infinity; the products go in the pairs of xyzz_add_affine (G1's paired
+// product)
+template <class Acc, class C>
+__device__ __forceinline__ void sm_add_affine(const Acc &a, const Affine<C> &q)
 {
     if (q.is_inf()) return;
-    const Fq52 zz = a.ld(2);
+    const C zz = a.ld(2);
     if (zz.is_zero()) {
-        a.set({q.x, q.y, Fq52::one(), Fq52::one()});
+        a.set({q.x, q.y, C::one(), C::one()});
         return;
     }
-    Fq52 u2, s2;
+    C u2, s2;
     mul2(q.x, zz, q.y, a.ld(3), u2, s2);
-    const Fq52 p = u2 - a.ld(0);
-    const Fq52 r = s2 - a.ld(1);
+    const C p = u2 - a.ld(0);
+    const C r = s2 - a.ld(1);
     if (p.is_zero()) {
-        a.set(r.is_zero() ? xyzz_from_affine_dbl(q) : Xyzz<Fq52>::inf());
+        a.set(r.is_zero() ? xyzz_from_affine_dbl(q) : Xyzz<C>::inf());
         return;
     }
-    Fq52 pp, rr, ppp, qq, y1ppp, ry, t;
+    C pp, rr, ppp, qq, y1ppp, ry, t;
     mul2(p, p, r, r, pp, rr);
     mul2(p, pp, a.ld(0), pp, ppp, qq);
     mul2(a.ld(3), ppp, a.ld(1), ppp, t, y1ppp);
     a.st(3, t);
-    const Fq52 ox = rr - ppp - dbl(qq);
+    const C ox = rr - ppp - dbl(qq);
     a.st(0, ox);
     mul2(r, qq - ox, a.ld(2), pp, ry, t);
     a.st(2, t);
     a.st(1, ry - y1ppp);
 }
 
-// acc_l1_body for G1 with the accumulator in shared memory (same runs, same
-// flushes, same results)
+// The same for G2, whose products are single calls: each product right before
+// its first use keeps fewer values live (167 registers and no spills at the
+// 3-block budget, against 104 B of spills in the paired order)
 template <int BS>
-__device__ __forceinline__ void acc_l1_body_g1s(const uint32_t *__restrict__ offsets,
-                                                const uint32_t *__restrict__ entries,
-                                                const Affine<Fq> *__restrict__ pts, uint32_t nb,
-                                                uint32_t k1, Xyzz<Fq> *__restrict__ partials,
-                                                Xyzz<Fq> *__restrict__ buckets, uint32_t t,
-                                                uint64_t *sm_block)
+__device__ __forceinline__ void sm_add_affine(const SmXyzzFq2<BS> &a, const Affine<Fq2> &q)
 {
+    if (q.is_inf()) return;
+    const Fq2 zz = a.ld(2);
+    if (zz.is_zero()) {
+        a.set({q.x, q.y, Fq2::one(), Fq2::one()});
+        return;
+    }
+    const Fq2 p = q.x * zz - a.ld(0);
+    const Fq2 r = q.y * a.ld(3) - a.ld(1);
+    if (p.is_zero()) {
+        a.set(r.is_zero() ? xyzz_from_affine_dbl(q) : Xyzz<Fq2>::inf());
+        return;
+    }
+    const Fq2 pp = sqr(p);
+    const Fq2 ppp = p * pp;
+    a.st(3, a.ld(3) * ppp);
+    const Fq2 qq = a.ld(0) * pp;
+    const Fq2 ox = sqr(r) - ppp - dbl(qq);
+    a.st(0, ox);
+    const Fq2 y1ppp = a.ld(1) * ppp;
+    a.st(1, r * (qq - ox) - y1ppp);
+    a.st(2, a.ld(2) * pp);
+}
+
+// Level 1: thread t sums the fixed segment [t K1, (t+1) K1) of the sorted
+// entries, split into runs at bucket boundaries, so every lane of a warp does
+// the same number of mixed additions whatever the bucket sizes.  A run that is
+// a whole bucket is written to the bucket; the segment's first / last run, when
+// its bucket continues outside the segment, goes to partial slot 2t / 2t + 1.
+template <class Acc, class F>
+__device__ __forceinline__ void acc_l1_body(const uint32_t *__restrict__ offsets,
+                                            const uint32_t *__restrict__ entries,
+                                            const Affine<F> *__restrict__ pts, uint32_t nb,
+                                            uint32_t k1, Xyzz<F> *__restrict__ partials,
+                                            Xyzz<F> *__restrict__ buckets, uint32_t t, const Acc &acc)
+{
+    using C = decltype(acc.ld(0));
     const uint32_t total = offsets[nb];
     const uint64_t beg64 = uint64_t(t) * k1;
     if (beg64 >= total) return;
@@ -486,16 +505,18 @@ __device__ __forceinline__ void acc_l1_body_g1s(const uint32_t *__restrict__ off
     uint32_t b = upper_bound_u32(offsets, nb + 1, beg) - 1; // offsets[b] <= beg < offsets[b + 1]
     uint32_t bstart = offsets[b], bend = offsets[b + 1];
     bool first = true;
-    const SmXyzz52<BS> acc{sm_block + threadIdx.x};
-    acc.set(Xyzz<Fq52>::inf());
+    acc.set(Xyzz<C>::inf());
+    // one flat loop with the same trip count in every lane keeps the additions
+    // converged; the flush at a bucket boundary is a short divergent branch
     for (uint32_t j = beg; j < end; ++j) {
         if (j == bend) {
             if (bstart >= beg)
-                buckets[b] = stx(acc.get());
+                buckets[b] = acc.out(); // the bucket started and ended inside the segment
             else
-                partials[2ull * t] = stx(acc.get());
+                partials[2ull * t] = acc.out(); // first run, bucket began in an earlier segment
             first = false;
-            acc.set(Xyzz<Fq52>::inf());
+            acc.set(Xyzz<C>::inf());
+            // next nonempty bucket: usually adjacent, else search
             ++b;
             int steps = 0;
             while (offsets[b + 1] <= j && steps < 8) {
@@ -507,35 +528,23 @@ __device__ __forceinline__ void acc_l1_body_g1s(const uint32_t *__restrict__ off
             bend = offsets[b + 1];
         }
         const uint32_t e = entries[j];
-        Affine<Fq52> p = lda(pts[e & 0x7fffffffu]);
+        typename Acc::point p = Acc::load(pts[e & 0x7fffffffu]);
         if (e >> 31) p = affine_neg(p);
-        sm_add_affine<BS>(acc, p);
+        sm_add_affine(acc, p);
     }
     if (bstart >= beg && bend <= end)
-        buckets[b] = stx(acc.get());
+        buckets[b] = acc.out();
     else
-        partials[2ull * t + (first ? 0 : 1)] = stx(acc.get());
+        partials[2ull * t + (first ? 0 : 1)] = acc.out();
 }
 
-// Level 1 kernels.  G1 (FP64 field, paired products passed by value, the
-// accumulator in shared memory) gets a 3-blocks-per-SM register budget: measured
-// against the compiler's own choice (184 registers, 2 blocks) and a 4-block
-// budget (128 registers, more spills), it is the fastest from 2^16 to 2^20
-// points, uniform and sparse.  With the accumulator in registers the same budget
-// spilled 100 B per thread and the kernel took 1.4% longer at 2^20; with it in
-// shared memory a 4-block budget still spills (124 B) and is no faster.  G2
-// keeps the compiler's choice (232 registers, 2 blocks per SM; a 3-block budget
-// spills 284 B per thread and is no faster).
-template <class F>
-__global__ void __launch_bounds__(128) k_acc_l1(const uint32_t *__restrict__ offsets,
-                                                 const uint32_t *__restrict__ entries,
-                                                 const Affine<F> *__restrict__ pts, uint32_t nb,
-                                                 uint32_t k1, Xyzz<F> *__restrict__ partials,
-                                                 Xyzz<F> *__restrict__ buckets)
-{
-    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x);
-}
-
+// Level 1 kernels, 3 blocks of 128 threads per SM.  G1 (FP64 field, paired
+// products passed by value): measured against the compiler's own register
+// choice (184 registers, 2 blocks) and a 4-block budget (128 registers, 124 B of
+// spills), the fastest from 2^16 to 2^20 points, uniform and sparse.  G2 (integer
+// pipe): 167 registers without spills, against 232 at 2 blocks per SM before the
+// accumulator moved to shared memory (a 4-block budget spills 232 B and is no
+// faster).
 __global__ void __launch_bounds__(128, 3) k_acc_l1_g1(const uint32_t *__restrict__ offsets,
                                                        const uint32_t *__restrict__ entries,
                                                        const Affine<Fq> *__restrict__ pts,
@@ -544,8 +553,20 @@ __global__ void __launch_bounds__(128, 3) k_acc_l1_g1(const uint32_t *__restrict
                                                        Xyzz<Fq> *__restrict__ buckets)
 {
     __shared__ uint64_t sm[20 * 128];
-    acc_l1_body_g1s<128>(offsets, entries, pts, nb, k1, partials, buckets,
-                         blockIdx.x * blockDim.x + threadIdx.x, sm);
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x,
+                SmXyzz52<128>{sm + threadIdx.x});
+}
+
+__global__ void __launch_bounds__(128, 3) k_acc_l1_g2(const uint32_t *__restrict__ offsets,
+                                                       const uint32_t *__restrict__ entries,
+                                                       const Affine<Fq2> *__restrict__ pts,
+                                                       uint32_t nb, uint32_t k1,
+                                                       Xyzz<Fq2> *__restrict__ partials,
+                                                       Xyzz<Fq2> *__restrict__ buckets)
+{
+    __shared__ uint32_t sm[64 * 128];
+    acc_l1_body(offsets, entries, pts, nb, k1, partials, buckets, blockIdx.x * blockDim.x + threadIdx.x,
+                SmXyzzFq2<128>{sm + threadIdx.x});
 }
 
 // Level 1 of several MSMs of one group in one launch (a batch's MSMs, any sizes):
@@ -574,20 +595,20 @@ __device__ __forceinline__ AccItem<F> acc_list_item(const AccItem<F> *items, int
     return items[lo];
 }
 
-template <class F>
-__global__ void __launch_bounds__(128) k_acc_l1_list(const AccItem<F> *items, int n_items)
-{
-    const AccItem<F> it = acc_list_item(items, n_items);
-    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
-                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x);
-}
-
 __global__ void __launch_bounds__(128, 3) k_acc_l1_g1_list(const AccItem<Fq> *items, int n_items)
 {
     __shared__ uint64_t sm[20 * 128];
     const AccItem<Fq> it = acc_list_item(items, n_items);
-    acc_l1_body_g1s<128>(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
-                         (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x, sm);
+    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
+                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x, SmXyzz52<128>{sm + threadIdx.x});
+}
+
+__global__ void __launch_bounds__(128, 3) k_acc_l1_g2_list(const AccItem<Fq2> *items, int n_items)
+{
+    __shared__ uint32_t sm[64 * 128];
+    const AccItem<Fq2> it = acc_list_item(items, n_items);
+    acc_l1_body(it.offsets, it.entries, it.pts, it.nb, it.k1, it.partials, it.buckets,
+                (blockIdx.x - it.first_block) * blockDim.x + threadIdx.x, SmXyzzFq2<128>{sm + threadIdx.x});
 }
 
 // One group of k2 pieces (spaced `stride` pieces apart) of one bucket; the
@@ -979,7 +1000,7 @@ int acc_level1_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, cudaStream_t s
             offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
             a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     else
-        k_acc_l1<F><<<blocks_for(segs, 128), 128, 0, st>>>(
+        k_acc_l1_g2<<<blocks_for(segs, 128), 128, 0, st>>>(
             offsets, s.entries.as<uint32_t>(), bs.pts.as<Affine<F>>(), sh.nb, uint32_t(sh.k1),
             a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
     NKR_CHECK_LAUNCH();
@@ -1014,7 +1035,7 @@ int acc_level1_list_t(const MsmAccJob *jobs, int n, void *items_host, void *item
     if constexpr (std::is_same<F, Fq>::value)
         k_acc_l1_g1_list<<<unsigned(blocks), 128, 0, st>>>(d, n);
     else
-        k_acc_l1_list<F><<<unsigned(blocks), 128, 0, st>>>(d, n);
+        k_acc_l1_g2_list<<<unsigned(blocks), 128, 0, st>>>(d, n);
     NKR_CHECK_LAUNCH();
     return NKR_B200_OK;
 }
