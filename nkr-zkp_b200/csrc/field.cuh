@@ -510,8 +510,9 @@ __device__ __forceinline__ uint32_t p2_word(int k)
 // arithmetic closed over the type.  It is the compute type of the G2 bucket
 // reduction levels, whose long dependent chains gain from the shorter product
 // (at 2^18 points: first level 0.41 -> 0.36 ms, block levels 1.50 -> 1.22 ms);
-// the G2 accumulation keeps Fq2, where the larger product body costs registers
-// (255, with spills) and ran 4% slower.
+// the G2 accumulation keeps Fq2, where the larger product body costs registers:
+// 255 with spills at 2 blocks per SM (4% slower), 100 B of spills at the 3-block
+// budget of the shared-memory accumulator (3.86 instead of 3.25 ms at 2^18).
 struct Fq2L : Fq2 {
     Fq2L() = default;
     __device__ __forceinline__ Fq2L(const Fq2 &a) : Fq2(a) {}
