@@ -56,19 +56,20 @@ METRIC = "Groth16 prove ms @2^20 constraints (bit-exact)"
 # DRAM read + write bytes per (point, digit) entry of the G1 accumulation kernel,
 # from an ncu capture at 2^18 points (a 2^20 capture would hold ~6 GB of keys on
 # the device); traffic grows with entries (one random base gather per entry)
-TRAFFIC_PER_ENTRY = (439.725568e6 + 21.505024e6) / 3932125   # 117.3 B per entry
+TRAFFIC_PER_ENTRY = (439.882752e6 + 20.989440e6) / 3932125   # 117.2 B per entry
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_acc_l1_g1 on the "
-                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 117.3 B "
+                  "2^18-point uniform G1 MSM of --mode kernels (3,932,125 entries), 117.2 B "
                   "per entry, scaled by this launch's entries")
-# Thread instructions per 52-bit-limb Fq product: ncu smsp__inst_executed.sum x 32 over
-# the products of nkr_b200_bench_mul's FP64 form (7,027,636,736 warp instructions for
+# Thread instructions per 52-bit-limb Fq product in the lazily reduced form the G1
+# accumulation runs: ncu smsp__inst_executed.sum x 32 over the products of
+# nkr_b200_bench_mul's variant 4 (6,603,139,584 warp instructions for
 # 148 x 16 x 256 threads x 256 x 4 = 620,756,992 products).
-INSTR_PER_PRODUCT = 7027636736 * 32 / 620756992   # 362.3
+INSTR_PER_PRODUCT = 6603139584 * 32 / 620756992   # 340.4
 # Pipe counters of k_acc_l1_g1 from one ncu launch (2^18-point uniform G1 MSM of
 # --mode kernels; profiles/k_acc_l1_g1_msm_2_18.md); percentages of peak.
-ACC_NCU = {"issue_active_pct": 58.83, "fp64_pipe_pct": 41.23, "alu_pipe_pct": 53.02,
-           "fmaheavy_pipe_pct": 20.13, "warps_active_per_sm": 10.69, "registers": 168,
-           "stall_per_issue": {"wait": 0.80, "not_selected": 0.76, "math_pipe_throttle": 0.67,
+ACC_NCU = {"issue_active_pct": 59.27, "fp64_pipe_pct": 40.11, "alu_pipe_pct": 56.05,
+           "fmaheavy_pipe_pct": 18.69, "warps_active_per_sm": 10.68, "registers": 168,
+           "stall_per_issue": {"wait": 0.75, "not_selected": 0.75, "math_pipe_throttle": 0.66,
                                "long_scoreboard": 0.55},
            "source": "ncu --metrics ... -k regex:k_acc_l1_g1 -c 1, --clock-control none"}
 
@@ -441,10 +442,10 @@ def run_b200(args):
     # the G1 accumulation runs: every SM issues 4 warp instructions per cycle and one
     # product costs INSTR_PER_PRODUCT thread instructions (ncu), so no kernel built
     # from these products exceeds SMs x 4 x 32 x f_sm / INSTR_PER_PRODUCT products/s.
-    # The best register-resident microbenchmark of the same product (itself at ~58%
+    # The best register-resident microbenchmark of the same product (itself at ~60%
     # issue) is reported beside it.
     peak_int, _ = ctx.bench_mul(1)
-    peak_fp64, _ = ctx.bench_mul(1 | (3 << 8))
+    peak_fp64, _ = ctx.bench_mul(1 | (4 << 8))  # the lazily reduced FP64 form
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     f_sm = (clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0) * 1e6
     issue_peak = sms * 4 * 32 * f_sm / INSTR_PER_PRODUCT
@@ -478,7 +479,7 @@ def run_b200(args):
                                "fp64_52bit": round(peak_fp64 / 1e9, 2),
                                "frac_of_best": round(achieved / max(peak_int, peak_fp64), 3),
                                "note": "register-resident product chains (nkr_b200_bench_mul), "
-                                       "issue active ~58% themselves"},
+                                       "issue active ~60% themselves"},
                 "ncu": ACC_NCU,
                 "units_per_launch": {"entries": st["entries"], "fq_muls": muls,
                                      "window_bits": st["window_bits"], "windows": st["windows"],
@@ -917,7 +918,7 @@ def run_kernels(args):
     peaks = _measured_peaks()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     fr_peak, _ = ctx.bench_mul(0)
-    fq_peak = max(ctx.bench_mul(1)[0], ctx.bench_mul(1 | (3 << 8))[0])
+    fq_peak = max(ctx.bench_mul(1)[0], ctx.bench_mul(1 | (4 << 8))[0])
     clocks = ClockSampler(0)
     clocks.start()
     launches0 = nk.launch_count()

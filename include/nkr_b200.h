@@ -375,7 +375,8 @@ int nkr_b200_group_op(nkr_b200_ctx *ctx, int group, int op, const void *a, const
                       void *out, uint64_t n);
 /* Throughput microbenchmark of the Montgomery product: field 0 Fr, 1 Fq; bits
  * 8.. select the formulation (0 the library's product, 1 a 64-bit-accumulation
- * variant, 2 squaring).  Returns products per second and the best kernel ms. */
+ * variant, 2 squaring, 3 the 52-bit-limb FP64 product, 4 the same lazily
+ * reduced to [0, 2p)).  Returns products per second and the best kernel ms. */
 int nkr_b200_bench_mul(nkr_b200_ctx *ctx, int field, double *muls_per_s, double *ms);
 
 /* ---- setup ------------------------------------------------------------------ */

@@ -13,7 +13,8 @@
 // the offsets' bit patterns are the integers; the 25 limb products of a x b
 // are independent, columns are summed as 64-bit integers and the offsets are
 // removed once per column.  The reduction is word-serial Montgomery with
-// 52-bit words (q = t * (-p^-1) mod 2^52 by integer multiply; q * p by FMA).
+// 52-bit words (q = t * (-p^-1) mod 2^52 by integer multiply; q * p by FMA,
+// of whose lowest limb product only the high half is formed).
 //
 // Representation: limbs are uint64 integers < 2^52, values canonical (< p),
 // Montgomery form with R' = 2^260.  In memory these values are stored in the
@@ -29,6 +30,7 @@ namespace nkr {
 
 struct Fq52 {
     uint64_t l[5];
+    static constexpr bool kCanonical = true; // products end with the conditional subtraction
     __device__ __forceinline__ static Fq52 zero() { return {{0, 0, 0, 0, 0}}; }
     // 2^260 mod p
     __device__ __forceinline__ static Fq52 one()
@@ -63,6 +65,20 @@ __host__ __device__ constexpr uint64_t p_limb(int k)
                     : 0x30644e72e131ull;
 }
 constexpr uint64_t kPinv = 0x20782e4866389ull;
+// 2p in 52-bit limbs
+__host__ __device__ constexpr uint64_t p2_limb(int k)
+{
+    return k == 0 ? 0x1182db0f9fa8eull
+           : k == 1 ? 0x22d0e3951a784ull
+           : k == 2 ? 0x302b0bb2f02d5ull
+           : k == 3 ? 0x405370a08b6d0ull
+                    : 0x60c89ce5c263ull;
+}
+template <int M> // M p in limbs, M = 1 or 2
+__host__ __device__ constexpr uint64_t mp_limb(int k)
+{
+    return M == 1 ? p_limb(k) : p2_limb(k);
+}
 
 __device__ __forceinline__ double to_double(uint64_t v) // v < 2^52, exact
 {
@@ -81,14 +97,15 @@ __device__ __forceinline__ void mul_wide(double a, double b, uint64_t &lo_b, uin
 }
 
 
-// s (five 52-bit limbs, value < 2p) minus p when s >= p
-__device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
+// s (five 52-bit limbs, value < 2 M p) minus M p when s >= M p
+template <int M>
+__device__ __forceinline__ void sub_mp_if_ge(uint64_t *s)
 {
     uint64_t d[5];
     int64_t borrow = 0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-        const int64_t t = int64_t(s[k]) - int64_t(p_limb(k)) + borrow;
+        const int64_t t = int64_t(s[k]) - int64_t(mp_limb<M>(k)) + borrow;
         d[k] = uint64_t(t) & kMask;
         borrow = t >> 52;
     }
@@ -97,6 +114,8 @@ __device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
         for (int k = 0; k < 5; ++k) s[k] = d[k];
     }
 }
+// s (value < 2p) minus p when s >= p
+__device__ __forceinline__ void sub_p_if_ge(uint64_t *s) { sub_mp_if_ge<1>(s); }
 
 } // namespace f52
 
@@ -106,12 +125,15 @@ __device__ __forceinline__ void sub_p_if_ge(uint64_t *s)
 #define NKR_MUL52_ATTR __forceinline__
 #endif
 
-// N independent products r[k] = a[k] b[k] 2^-260 mod p, canonical; each needs
-// a b < 2^260 p (true for a, b < 4p).  The N computations share no data, so the
-// scheduler interleaves their dependency chains (the word-serial reduction is
-// one long chain per product).
-template <int N>
-__device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *const *b, Fq52 *const *r)
+// N independent products r[k] = a[k] b[k] 2^-260 mod p.  The word-serial
+// Montgomery result t = (a b + q p) / 2^260 with q < 2^260 is below
+// a b / 2^260 + p: for a, b < 2p that is under 1.05 p, so the canonical type
+// (T::kCanonical) ends with one conditional subtraction of p and the lazily
+// reduced type (Fq52L, values in [0, 2p)) skips it.  The N computations share no
+// data, so the scheduler interleaves their dependency chains (the word-serial
+// reduction is one long chain per product).
+template <int N, class T>
+__device__ __forceinline__ void mul52_body(const T *const *a, const T *const *b, T *const *r)
 {
     using namespace f52;
     double ad[N][5], bd[N][5], pd[5];
@@ -162,9 +184,12 @@ __device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *con
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             uint64_t lo, hi;
-            mul_wide(q[k], pd[0], lo, hi);
-            t[k] += lo - kBias52; // now 0 mod 2^52
-            C[k][i + 1] += hi + (t[k] >> 52);
+            // t + q p0 is 0 mod 2^52 and the low 52 bits of t and of q p0 are
+            // each below 2^52, so they sum to 0 (t's are 0) or to 2^52: the carry
+            // into the next column needs only the high half of q p0 (one FMA
+            // instead of two FMAs and a subtraction)
+            hi = static_cast<uint64_t>(__double_as_longlong(__fma_rz(q[k], pd[0], 0x1p104)));
+            C[k][i + 1] += hi + (t[k] >> 52) + ((t[k] & kMask) != 0 ? 1u : 0u);
 #pragma unroll
             for (int j = 1; j < 5; ++j) {
                 mul_wide(q[k], pd[j], lo, hi);
@@ -188,7 +213,7 @@ __device__ __forceinline__ void mul52_body(const Fq52 *const *a, const Fq52 *con
             r[k]->l[j - 5] = v & kMask;
             carry = v >> 52;
         }
-        sub_p_if_ge(r[k]->l); // the result is below 2p
+        if constexpr (T::kCanonical) sub_p_if_ge(r[k]->l); // the result is below 2p
     }
 }
 
@@ -290,6 +315,123 @@ __device__ __forceinline__ Fq52 operator-(const Fq52 &a, const Fq52 &b)
 
 __device__ __forceinline__ Fq52 neg(const Fq52 &a) { return Fq52::zero() - a; }
 __device__ __forceinline__ Fq52 dbl(const Fq52 &a) { return a + a; }
+
+// ---------------------------------------------------------------------------
+// Fq52L: the same limbs and R' domain, lazily reduced -- every value is in
+// [0, 2p), not canonical.  A product of two such values is already below
+// 1.05 p (mul52_body), so it skips the conditional subtraction of p that ends a
+// canonical product (about 40 of its 362 instructions); additions and
+// subtractions work modulo 2p at the cost of their canonical forms.  Zero tests
+// accept 0 and p.  MSM kernels compute in this type and canonicalise once, when a
+// value leaves for memory (canon()).
+// ---------------------------------------------------------------------------
+struct Fq52L {
+    uint64_t l[5];
+    static constexpr bool kCanonical = false;
+    Fq52L() = default;
+    __device__ __forceinline__ Fq52L(const Fq52 &c) // a canonical value is in range
+    {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) l[k] = c.l[k];
+    }
+    __device__ __forceinline__ static Fq52L zero() { return Fq52::zero(); }
+    __device__ __forceinline__ static Fq52L one() { return Fq52::one(); }
+    __device__ __forceinline__ bool is_zero() const // 0 or p
+    {
+        return (l[0] | l[1] | l[2] | l[3] | l[4]) == 0 ||
+               ((l[0] ^ f52::p_limb(0)) | (l[1] ^ f52::p_limb(1)) | (l[2] ^ f52::p_limb(2)) |
+                (l[3] ^ f52::p_limb(3)) | (l[4] ^ f52::p_limb(4))) == 0;
+    }
+    __device__ __forceinline__ Fq52 canon() const
+    {
+        Fq52 r;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) r.l[k] = l[k];
+        f52::sub_p_if_ge(r.l);
+        return r;
+    }
+    __device__ __forceinline__ bool operator==(const Fq52L &o) const { return canon() == o.canon(); }
+    __device__ __forceinline__ bool operator!=(const Fq52L &o) const { return !(*this == o); }
+};
+
+__device__ NKR_MUL52_ATTR Fq52L mul52L(Fq52L a, Fq52L b)
+{
+    Fq52L r;
+    const Fq52L *pa[1] = {&a}, *pb[1] = {&b};
+    Fq52L *pr[1] = {&r};
+    mul52_body<1>(pa, pb, pr);
+    return r;
+}
+
+struct Fq52LPair {
+    Fq52L x, y;
+};
+
+// (a b, c d) in one call, lazily reduced (as mul52x2v)
+__device__ NKR_MUL52_ATTR Fq52LPair mul52Lx2v(Fq52L a, Fq52L b, Fq52L c, Fq52L d)
+{
+    Fq52LPair r;
+    const Fq52L *pa[2] = {&a, &c}, *pb[2] = {&b, &d};
+    Fq52L *pr[2] = {&r.x, &r.y};
+    mul52_body<2>(pa, pb, pr);
+    return r;
+}
+
+__device__ __forceinline__ Fq52L operator*(const Fq52L &a, const Fq52L &b) { return mul52L(a, b); }
+__device__ __forceinline__ Fq52L sqr(const Fq52L &a) { return mul52L(a, a); }
+
+__device__ __forceinline__ void mul2(const Fq52L &a, const Fq52L &b, const Fq52L &c, const Fq52L &d,
+                                     Fq52L &x, Fq52L &y)
+{
+    const Fq52LPair r = mul52Lx2v(a, b, c, d);
+    x = r.x;
+    y = r.y;
+}
+template <>
+struct HasPairedMul<Fq52L> {
+    static constexpr bool value = true;
+};
+
+// (a + b) mod 2p for a, b in [0, 2p)
+__device__ __forceinline__ Fq52L operator+(const Fq52L &a, const Fq52L &b)
+{
+    Fq52L r;
+    uint64_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const uint64_t t = a.l[k] + b.l[k] + c;
+        r.l[k] = t & f52::kMask;
+        c = t >> 52;
+    }
+    f52::sub_mp_if_ge<2>(r.l);
+    return r;
+}
+
+// (a - b) mod 2p for a, b in [0, 2p)
+__device__ __forceinline__ Fq52L operator-(const Fq52L &a, const Fq52L &b)
+{
+    Fq52L r;
+    int64_t br = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int64_t t = int64_t(a.l[k]) - int64_t(b.l[k]) + br;
+        r.l[k] = uint64_t(t) & f52::kMask;
+        br = t >> 52;
+    }
+    if (br) { // a < b: add 2p back
+        uint64_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const uint64_t t = r.l[k] + f52::p2_limb(k) + c;
+            r.l[k] = t & f52::kMask;
+            c = t >> 52;
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ Fq52L neg(const Fq52L &a) { return Fq52L::zero() - a; }
+__device__ __forceinline__ Fq52L dbl(const Fq52L &a) { return a + a; }
 
 // Fq2 = Fq[u] / (u^2 + 1) over Fq52 (Karatsuba, as Fq2 in field.cuh)
 struct Fq2x52 {

@@ -57,6 +57,13 @@ __device__ __forceinline__ Fq52 shfl_xor1(unsigned mask, const Fq52 &a)
     for (int j = 0; j < 5; ++j) r.l[j] = __shfl_xor_sync(mask, a.l[j], 1);
     return r;
 }
+__device__ __forceinline__ Fq52L shfl_xor1(unsigned mask, const Fq52L &a)
+{
+    Fq52L r;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) r.l[j] = __shfl_xor_sync(mask, a.l[j], 1);
+    return r;
+}
 __device__ __forceinline__ Fq2 shfl_xor1(unsigned mask, const Fq2 &a)
 {
     Fq2 r;
@@ -213,7 +220,7 @@ template <class F>
 struct MsmArith;
 template <>
 struct MsmArith<Fq> {
-    using type = Fq52;
+    using type = Fq52L;
 };
 template <>
 struct MsmArith<Fq2> {
@@ -259,10 +266,12 @@ struct BaseOf<Pair2<B>> {
     using type = B;
 };
 
-__device__ __forceinline__ Fq52 msm_in(const Fq &x) { return to52(x); }
-__device__ __forceinline__ Fq msm_out(const Fq52 &x) { return from52(x); }
-__device__ __forceinline__ Fq52 msm_enter(const Fq52 &x) { return r256_to_r260(x); }
-__device__ __forceinline__ Fq52 msm_leave(const Fq52 &x) { return r260_to_r256(x); }
+// G1 buffers hold canonical values; the lazily reduced compute values are
+// canonicalised on the way out
+__device__ __forceinline__ Fq52L msm_in(const Fq &x) { return to52(x); }
+__device__ __forceinline__ Fq msm_out(const Fq52L &x) { return from52(x.canon()); }
+__device__ __forceinline__ Fq52L msm_enter(const Fq52L &x) { return r256_to_r260(x.canon()); }
+__device__ __forceinline__ Fq52L msm_leave(const Fq52L &x) { return r260_to_r256(x.canon()); }
 __device__ __forceinline__ Fq2 msm_in(const Fq2 &x) { return x; }
 __device__ __forceinline__ Fq2 msm_out(const Fq2 &x) { return x; }
 __device__ __forceinline__ Fq2 msm_enter(const Fq2 &x) { return x; }
@@ -361,31 +370,31 @@ struct LoadLeaders {
 // spills (6% faster at 2^18).  Layout: structure of arrays, word w of thread i
 // at w * BS + i, so a warp's accesses are conflict-free.
 //
-// G1: Fq52 coordinates (5 x 64-bit words), R' domain throughout.
+// G1: Fq52L coordinates (5 x 64-bit words, lazily reduced), R' domain throughout.
 template <int BS>
 struct SmXyzz52 {
-    using point = Affine<Fq52>;
+    using point = Affine<Fq52L>;
     uint64_t *s; // the block's area + threadIdx.x; 20 words per thread
-    __device__ __forceinline__ Fq52 ld(int f) const
+    __device__ __forceinline__ Fq52L ld(int f) const
     {
-        Fq52 v;
+        Fq52L v;
 #pragma unroll
         for (int j = 0; j < 5; ++j) v.l[j] = s[(f * 5 + j) * BS];
         return v;
     }
-    __device__ __forceinline__ void st(int f, const Fq52 &v) const
+    __device__ __forceinline__ void st(int f, const Fq52L &v) const
     {
 #pragma unroll
         for (int j = 0; j < 5; ++j) s[(f * 5 + j) * BS] = v.l[j];
     }
-    __device__ __forceinline__ void set(const Xyzz<Fq52> &a) const
+    __device__ __forceinline__ void set(const Xyzz<Fq52L> &a) const
     {
         st(0, a.x);
         st(1, a.y);
         st(2, a.zz);
         st(3, a.zzz);
     }
-    __device__ __forceinline__ Xyzz<Fq> out() const { return stx(Xyzz<Fq52>{ld(0), ld(1), ld(2), ld(3)}); }
+    __device__ __forceinline__ Xyzz<Fq> out() const { return stx(Xyzz<Fq52L>{ld(0), ld(1), ld(2), ld(3)}); }
     __device__ __forceinline__ static point load(const Affine<Fq> &p) { return lda(p); }
 };
 

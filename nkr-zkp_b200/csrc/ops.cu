@@ -110,7 +110,8 @@ __global__ void k_group_op(int op, const F *a, const F *b, F *out, uint64_t n)
 
 // Each thread runs 4 independent product chains; the result is stored so the
 // work cannot be eliminated.  variant 0: operator* (64-bit accumulation CIOS),
-// 1: mont_mul_cc (PTX carry-chain CIOS), 2: squaring.
+// 1: mont_mul_cc (PTX carry-chain CIOS), 2: squaring; k_bench_mul52 below is
+// variant 3 (the 52-bit-limb FP64 product, canonical) and 4 (lazily reduced).
 constexpr int kBenchIters = 256;
 template <class P, int V>
 __global__ void __launch_bounds__(256) k_bench_mul(const Fp<P> *seed, Fp<P> *sink)
@@ -157,19 +158,43 @@ __global__ void k_check_52(const Fq *a, const Fq *b, uint32_t *bad, int n)
     if (r != a[i] * b[i]) atomicAdd(bad, 1u);
 }
 
+// The lazily reduced product (values in [0, 2p)) agrees with the canonical one
+// once canonicalised, also when an input is in [p, 2p).
+__global__ void k_check_52l(const Fq *a, const Fq *b, uint32_t *bad, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Fq52 x = to52(a[i]), y = to52(b[i]);
+    Fq52L xl = x, yl = y;
+    const Fq52 want = mul52(x, y);
+    if ((xl * yl).canon() != want) atomicAdd(bad, 1u);
+    xl = xl + Fq52L(Fq52{{f52::p_limb(0), f52::p_limb(1), f52::p_limb(2), f52::p_limb(3), f52::p_limb(4)}});
+    if ((xl * yl).canon() != want) atomicAdd(bad, 1u);
+}
+
+template <class T>
+__device__ __forceinline__ Fq bench52_out(const T &x)
+{
+    if constexpr (T::kCanonical)
+        return from52(x);
+    else
+        return from52(x.canon());
+}
+
+template <class T>
 __global__ void __launch_bounds__(256) k_bench_mul52(const Fq *seed, Fq *sink)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    Fq52 a = to52(seed[i & 255]), b = to52(seed[(i + 1) & 255]), c = to52(seed[(i + 2) & 255]),
-         d = to52(seed[(i + 3) & 255]);
-    const Fq52 m = to52(seed[(i + 7) & 255]);
+    T a = Fq52(to52(seed[i & 255])), b = Fq52(to52(seed[(i + 1) & 255])),
+      c = Fq52(to52(seed[(i + 2) & 255])), d = Fq52(to52(seed[(i + 3) & 255]));
+    const T m = Fq52(to52(seed[(i + 7) & 255]));
     for (int k = 0; k < kBenchIters; ++k) {
-        a = mul52(a, m);
-        b = mul52(b, m);
-        c = mul52(c, m);
-        d = mul52(d, m);
+        a = a * m;
+        b = b * m;
+        c = c * m;
+        d = d * m;
     }
-    const Fq r = from52(a) + from52(b) + from52(c) + from52(d);
+    const Fq r = bench52_out(a) + bench52_out(b) + bench52_out(c) + bench52_out(d);
     if (r.v[0] == 0x12345678u) sink[i] = r;
 }
 
@@ -244,7 +269,7 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
     float best = 1e30f;
     const int variant = field >> 8;
     field &= 0xff;
-    if (variant == 1 || variant == 3) {
+    if (variant == 1 || variant == 3 || variant == 4) {
         // the alternative product must agree with operator* before it is timed
         DevBuf bad;
         NKR_TRY(bad.alloc(4, "bench check"));
@@ -252,8 +277,10 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
         if (variant == 1)
             k_check_wide<FqParams><<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1,
                                                        bad.as<uint32_t>(), 255);
-        else
+        else if (variant == 3)
             k_check_52<<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1, bad.as<uint32_t>(), 255);
+        else
+            k_check_52l<<<1, 256, 0, st>>>(seed.as<Fq>(), seed.as<Fq>() + 1, bad.as<uint32_t>(), 255);
         NKR_CHECK_LAUNCH();
         uint32_t nbad = 0;
         NKR_CUDA(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, st));
@@ -269,7 +296,9 @@ int bench_mul_device(int field, int sm_count, double *muls_per_s, double *ms, cu
         else if (variant == 1)
             k_bench_mul<FqParams, 1><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         else if (variant == 3)
-            k_bench_mul52<<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+            k_bench_mul52<Fq52><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
+        else if (variant == 4)
+            k_bench_mul52<Fq52L><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         else
             k_bench_mul<FqParams, 2><<<blocks, 256, 0, st>>>(seed.as<Fq>(), sink.as<Fq>());
         NKR_CHECK_LAUNCH();

@@ -126,3 +126,8 @@ def test_mul_throughput_positive(ctx):
     for field in (0, 1):
         rate, ms = ctx.bench_mul(field)
         assert rate > 1e9 and ms > 0
+    # the FP64 forms check themselves against the library product before timing
+    # (the lazily reduced one also with an input in [p, 2p))
+    for variant in (3, 4):
+        rate, ms = ctx.bench_mul(1 | (variant << 8))
+        assert rate > 1e9 and ms > 0
