@@ -55,7 +55,11 @@ struct MsmShape {
     bool folded = false;
     uint32_t B = 0;  // buckets per set: 2^(c-1)
     uint32_t nb = 0; // total buckets: folded ? B : W * B
-    int k1 = 32;     // entries per level-1 segment (mixed additions per thread; 8-32 by size)
+    // entries per level-1 segment (mixed additions per thread).  Measured slower
+    // at 2^16 points: 8 or 16 (level 1 shorter, fix-ups and the first reduction
+    // level longer); at 2^20: 32-48 sized to whole waves of the kernel (prove
+    // 18.60 -> 18.79 ms)
+    int k1 = 32;
     int k2 = 16;     // fan-in of the fix-up levels (8 and 4 measured no faster in a prove)
     uint64_t entries_max() const { return uint64_t(W) * n; }
     uint64_t segments_max() const { return (entries_max() + k1 - 1) / k1; }
