@@ -150,14 +150,17 @@ __device__ __forceinline__ unsigned equal_scalar_lanes(unsigned mask, const Fr &
 }
 
 __global__ void k_digits_count(const Fr *__restrict__ scalars, const uint32_t *__restrict__ gather,
-                               uint64_t n, int c, int W, bool folded, uint32_t B,
-                               Fr *__restrict__ canon, uint32_t *__restrict__ counts)
+                               const uint32_t *__restrict__ class_of, uint64_t n, int c, int W,
+                               bool folded, uint32_t B, Fr *__restrict__ canon,
+                               uint32_t *__restrict__ counts)
 {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = i < n;
     Fr s = Fr::zero();
     if (live) {
-        s = from_mont(scalars[gather ? gather[i] : i]);
+        const uint64_t v = gather ? gather[i] : i;
+        // a class member's scalar is added by the class path (zero: no digits here)
+        if (!class_of || class_of[v] == kNoClass) s = from_mont(scalars[v]);
         canon[i] = s;
     }
     const int lane = threadIdx.x & 31;
@@ -1097,26 +1100,34 @@ int reduce_run(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, c
     return NKR_B200_OK;
 }
 
+// Fix-up levels of a level-1 accumulation with shape sh (segments, buckets,
+// k1, k2) whose bucket offsets are `offsets`: inputs spaced `stride` pieces
+// apart, groups of k2; one bucket has at most segs + 1 pieces, all buckets at
+// most 2 segs.
 template <class F>
-int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+int fixup_levels_t(const MsmShape &sh, const uint32_t *offsets, uint32_t *lead_off, uint32_t *scan_tmp,
+                   Xyzz<F> *partials, Xyzz<F> *buckets, cudaStream_t st)
 {
-    const MsmShape &sh = bs.shape;
     const uint64_t segs = sh.segments_max();
-    const uint32_t *offsets = s.offsets.as<uint32_t>();
-    // fix-up levels: inputs spaced `stride` pieces apart, groups of k2; one
-    // bucket has at most segs + 1 pieces, all buckets at most 2 segs
     const uint64_t k2 = uint64_t(sh.k2);
     for (uint64_t stride = 1; stride < segs + 1; stride *= k2) {
         NKR_TRY(scan_exclusive(LoadLeaders{offsets, uint32_t(sh.k1), uint32_t(stride), uint32_t(k2)},
-                               sh.nb, a.lead_off.as<uint32_t>(), a.scan_tmp.as<uint32_t>(), st));
+                               sh.nb, lead_off, scan_tmp, st));
         const uint64_t bound = 2 * segs / (stride * k2) + sh.nb + 1;
         const unsigned grid = std::min<unsigned>(blocks_for(bound, 128), kFixupBlocks);
-        k_acc_up<F><<<grid, 128, 0, st>>>(offsets, a.lead_off.as<uint32_t>(), sh.nb,
-                                                            uint32_t(sh.k1), a.partials.as<Xyzz<F>>(),
-                                                            a.buckets.as<Xyzz<F>>(), uint32_t(stride),
-                                                            uint32_t(k2));
+        k_acc_up<F><<<grid, 128, 0, st>>>(offsets, lead_off, sh.nb, uint32_t(sh.k1), partials, buckets,
+                                           uint32_t(stride), uint32_t(k2));
         NKR_CHECK_LAUNCH();
     }
+    return NKR_B200_OK;
+}
+
+template <class F>
+int acc_tail_t(const MsmBases &bs, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st)
+{
+    NKR_TRY(fixup_levels_t<F>(bs.shape, s.offsets.as<uint32_t>(), a.lead_off.as<uint32_t>(),
+                              a.scan_tmp.as<uint32_t>(), a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(),
+                              st));
     if (a.timing) NKR_CUDA(cudaEventRecord(a.ev_acc[2], st));
     // bucket reduction levels (G2 alone: on lane pairs)
     if constexpr (std::is_same<F, Fq2>::value)
@@ -1151,6 +1162,202 @@ int acc_alloc_t(MsmAcc &a, const MsmShape &sh)
     NKR_TRY(a.red_r2.alloc(red * sizeof(Xyzz<F>), "msm reduction"));
     NKR_TRY(a.scan_tmp.alloc(scan_scratch_words(sh.nb) * 4, "msm scan scratch"));
     NKR_TRY(a.result.alloc(192, "msm result"));
+    return NKR_B200_OK;
+}
+
+// --------------------------------------------------------------------------
+// repeated scalars: classes of equal witness values (msm.cuh)
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t scalar_hash(const Fr &s)
+{
+    return s.v[0] ^ (s.v[1] * 0x9e3779b9u) ^ (s.v[6] * 0x85ebca6bu) ^ (s.v[7] * 0xc2b2ae35u);
+}
+
+constexpr int kDedupProbes = 64; // a value not placed within this many slots stays a singleton
+
+// rep[i]: the representative variable of z_i's value (kNoClass for zero).  The
+// table holds variable indices (kNoClass = empty); a thread claims an empty
+// slot with atomicCAS or finds an equal value on its probe path.
+__global__ void k_dedup_insert(const Fr *__restrict__ z, uint64_t cols, uint32_t *__restrict__ table,
+                               uint64_t mask, uint32_t *__restrict__ rep)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cols) return;
+    const Fr s = z[i];
+    if (s.is_zero()) {
+        rep[i] = kNoClass;
+        return;
+    }
+    uint64_t h = scalar_hash(s) & mask;
+    uint32_t r = uint32_t(i);
+    for (int probe = 0; probe < kDedupProbes; ++probe) {
+        const uint32_t cur = atomicCAS(&table[h], kNoClass, uint32_t(i));
+        if (cur == kNoClass) break; // this variable represents its value
+        if (z[cur] == s) {
+            r = cur;
+            break;
+        }
+        h = (h + 1) & mask;
+    }
+    rep[i] = r;
+}
+
+// csize[r]: members of representative r (warp-aggregated per equal r)
+__global__ void k_dedup_count(const uint32_t *__restrict__ rep, uint64_t cols, uint32_t *__restrict__ csize)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t r = i < cols ? rep[i] : kNoClass;
+    const unsigned act = __ballot_sync(0xffffffffu, r != kNoClass);
+    if (r == kNoClass) return;
+    const unsigned peers = __match_any_sync(act, r);
+    if (int(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&csize[r], uint32_t(__popc(peers)));
+}
+
+// class ids for representatives of at least kClassMin members, first come first
+// served up to kClassMax; values[id] = the class's value
+__global__ void k_dedup_ids(const Fr *__restrict__ z, const uint32_t *__restrict__ rep,
+                            const uint32_t *__restrict__ csize, uint64_t cols, uint32_t *__restrict__ cid,
+                            Fr *__restrict__ values, uint32_t *__restrict__ nclass)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cols) return;
+    uint32_t id = kNoClass;
+    if (rep[i] == uint32_t(i) && csize[i] >= kClassMin) {
+        const uint32_t k = atomicAdd(nclass, 1u);
+        if (k < kClassMax) {
+            id = k;
+            values[k] = z[i];
+        }
+    }
+    cid[i] = id;
+}
+
+__global__ void k_dedup_mark(const uint32_t *__restrict__ rep, const uint32_t *__restrict__ cid,
+                             uint64_t cols, uint32_t *__restrict__ class_of)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cols) return;
+    const uint32_t r = rep[i];
+    class_of[i] = r == kNoClass ? kNoClass : cid[r];
+}
+
+// class members of a support: counts per class, then a scatter in class order
+// (warp-aggregated per equal class)
+__global__ void k_cls_count(const uint32_t *__restrict__ class_of, const uint32_t *__restrict__ gather,
+                            uint64_t n, uint32_t *__restrict__ counts)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t c = i < n ? class_of[gather ? gather[i] : i] : kNoClass;
+    const unsigned act = __ballot_sync(0xffffffffu, c != kNoClass);
+    if (c == kNoClass) return;
+    const unsigned peers = __match_any_sync(act, c);
+    if (int(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[c], uint32_t(__popc(peers)));
+}
+
+__global__ void k_cls_scatter(const uint32_t *__restrict__ class_of, const uint32_t *__restrict__ gather,
+                              uint64_t n, uint32_t *__restrict__ cursor, uint32_t *__restrict__ entries)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t c = i < n ? class_of[gather ? gather[i] : i] : kNoClass;
+    const unsigned act = __ballot_sync(0xffffffffu, c != kNoClass);
+    if (c == kNoClass) return;
+    const unsigned peers = __match_any_sync(act, c);
+    const int lane = int(threadIdx.x & 31), leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&cursor[c], uint32_t(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    entries[base + uint32_t(__popc(peers & ((1u << lane) - 1u)))] = uint32_t(i);
+}
+
+// a class sum as an affine base of the small MSM (storage form of the group's
+// MSM buffers: G1 in the R' domain; infinity as (0, one))
+__device__ __forceinline__ Affine<Fq> class_affine(const Xyzz<Fq52L> &s)
+{
+    if (s.is_inf()) return {from52(Fq52::zero()), from52(Fq52::one())};
+    const Affine<Fq52> a = xyzz_to_affine(Xyzz<Fq52>{s.x.canon(), s.y.canon(), s.zz.canon(), s.zzz.canon()});
+    return {from52(a.x), from52(a.y)};
+}
+__device__ __forceinline__ Affine<Fq2> class_affine(const Xyzz<Fq2> &s) { return xyzz_to_affine(s); }
+
+// S_c for every class: its pieces (level-1 runs and fix-up sums) added up and
+// normalised with one inversion per class
+template <class F>
+__global__ void __launch_bounds__(128) k_cls_finish(const uint32_t *__restrict__ offsets,
+                                                     const Xyzz<F> *__restrict__ partials,
+                                                     const Xyzz<F> *__restrict__ buckets, uint32_t k1,
+                                                     uint32_t nb, Affine<F> *__restrict__ sums)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nb) return;
+    using C = CF<F>;
+    sums[c] = class_affine(add_bucket_sum<C>(Xyzz<C>::inf(), offsets, partials, buckets, c, k1));
+}
+
+// acc += add for two libff-Jacobian points (X, Y, Z; Z = 0 is infinity) in the
+// library's Montgomery domain
+template <class F>
+__global__ void k_result_add(F *acc, const F *add)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    auto xyzz = [](const F *p) {
+        if (p[2].is_zero()) return Xyzz<F>::inf();
+        const F zz = sqr(p[2]);
+        return Xyzz<F>{p[0], p[1], zz, zz * p[2]};
+    };
+    const Xyzz<F> s = xyzz_add(xyzz(acc), xyzz(add));
+    if (s.is_inf()) {
+        acc[0] = F::zero();
+        acc[1] = F::one();
+        acc[2] = F::zero();
+        return;
+    }
+    const F zzz2 = sqr(s.zzz), zz2 = sqr(s.zz);
+    acc[0] = s.x * (s.zz * zzz2);
+    acc[1] = s.y * (zz2 * s.zz * zzz2);
+    acc[2] = s.zz * s.zzz;
+}
+
+template <class F>
+int class_acc_alloc_t(MsmClassAcc &a, uint64_t n)
+{
+    a.seg = MsmShape{};
+    a.seg.n = n;
+    a.seg.c = 1;
+    a.seg.W = 1;
+    a.seg.folded = true;
+    a.seg.B = kClassMax;
+    a.seg.nb = kClassMax;
+    const uint64_t segs = std::max<uint64_t>(a.seg.segments_max(), 1);
+    NKR_TRY(a.partials.alloc(2 * segs * sizeof(Xyzz<F>), "class partial sums"));
+    NKR_TRY(a.buckets.alloc(uint64_t(kClassMax) * sizeof(Xyzz<F>), "class sums"));
+    NKR_TRY(a.lead_off.alloc((kClassMax + 1) * 4ull, "class fix-up offsets"));
+    NKR_TRY(a.scan_tmp.alloc(scan_scratch_words(kClassMax) * 4, "class scan scratch"));
+    return NKR_B200_OK;
+}
+
+template <class F>
+int class_acc_issue_t(const MsmBases &b, const MsmClassSort &cs, MsmClassAcc &a, cudaStream_t st)
+{
+    const uint64_t segs = a.seg.segments_max();
+    const uint32_t *offsets = cs.offsets.as<uint32_t>();
+    if (segs) {
+        if constexpr (std::is_same<F, Fq>::value)
+            k_acc_l1_g1<<<blocks_for(segs, 128), 128, 0, st>>>(
+                offsets, cs.entries.as<uint32_t>(), b.pts.as<Affine<F>>(), kClassMax, uint32_t(a.seg.k1),
+                a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
+        else
+            k_acc_l1_g2<<<blocks_for(segs, 128), 128, 0, st>>>(
+                offsets, cs.entries.as<uint32_t>(), b.pts.as<Affine<F>>(), kClassMax, uint32_t(a.seg.k1),
+                a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>());
+        NKR_CHECK_LAUNCH();
+    }
+    NKR_TRY(fixup_levels_t<F>(a.seg, offsets, a.lead_off.as<uint32_t>(), a.scan_tmp.as<uint32_t>(),
+                              a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), st));
+    k_cls_finish<F><<<blocks_for(kClassMax, 128), 128, 0, st>>>(
+        offsets, a.partials.as<Xyzz<F>>(), a.buckets.as<Xyzz<F>>(), uint32_t(a.seg.k1), kClassMax,
+        a.small.pts.as<Affine<F>>());
+    NKR_CHECK_LAUNCH();
     return NKR_B200_OK;
 }
 
@@ -1314,14 +1521,14 @@ int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape)
 }
 
 int msm_sort_run(const MsmShape &sh, MsmSort &s, const void *scalars_dev, cudaStream_t st,
-                 const uint32_t *gather)
+                 const uint32_t *gather, const uint32_t *class_of)
 {
     const uint64_t n = sh.n;
     NKR_CUDA(cudaMemsetAsync(s.counts.p, 0, (sh.nb + 1) * 4, st));
     if (n) {
         k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>(
-            static_cast<const Fr *>(scalars_dev), gather, n, sh.c, sh.W, sh.folded, sh.B, s.canon.as<Fr>(),
-            s.counts.as<uint32_t>());
+            static_cast<const Fr *>(scalars_dev), gather, class_of, n, sh.c, sh.W, sh.folded, sh.B,
+            s.canon.as<Fr>(), s.counts.as<uint32_t>());
         NKR_CHECK_LAUNCH();
     }
     NKR_TRY(scan_exclusive(LoadU32{s.counts.as<uint32_t>()}, sh.nb, s.offsets.as<uint32_t>(),
@@ -1367,6 +1574,118 @@ int msm_run(const MsmBases &b, MsmScratch &s, const void *scalars_dev, void *out
 {
     NKR_TRY(msm_sort_run(b.shape, s.sort, scalars_dev, st, b.gather()));
     return msm_acc_run(b, s.sort, s.acc, out_dev, st);
+}
+
+int msm_dedup_alloc(MsmDedup &d, uint64_t cols)
+{
+    NKR_REQUIRE(cols < uint64_t(kNoClass), "witness of %llu variables too long for 32-bit indices",
+                (unsigned long long)cols);
+    d.cols = cols;
+    d.slots = 1;
+    while (d.slots < 2 * cols) d.slots <<= 1;
+    const uint64_t c = std::max<uint64_t>(cols, 1);
+    NKR_TRY(d.table.alloc(d.slots * 4, "dedup table"));
+    NKR_TRY(d.rep.alloc(c * 4, "dedup representatives"));
+    NKR_TRY(d.csize.alloc(c * 4, "dedup class sizes"));
+    NKR_TRY(d.cid.alloc(c * 4, "dedup class ids"));
+    NKR_TRY(d.class_of.alloc(c * 4, "dedup classes"));
+    NKR_TRY(d.values.alloc(uint64_t(kClassMax) * sizeof(Fr), "class values"));
+    NKR_TRY(d.nclass.alloc(4, "class count"));
+    return NKR_B200_OK;
+}
+
+int msm_dedup_run(MsmDedup &d, const void *z, cudaStream_t st)
+{
+    const uint64_t cols = d.cols;
+    NKR_CUDA(cudaMemsetAsync(d.table.p, 0xff, d.table.bytes, st));
+    NKR_CUDA(cudaMemsetAsync(d.csize.p, 0, d.csize.bytes, st));
+    NKR_CUDA(cudaMemsetAsync(d.values.p, 0, d.values.bytes, st));
+    NKR_CUDA(cudaMemsetAsync(d.nclass.p, 0, 4, st));
+    if (!cols) return NKR_B200_OK;
+    const Fr *zf = static_cast<const Fr *>(z);
+    const unsigned g = blocks_for(cols, 256);
+    k_dedup_insert<<<g, 256, 0, st>>>(zf, cols, d.table.as<uint32_t>(), d.slots - 1, d.rep.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    k_dedup_count<<<g, 256, 0, st>>>(d.rep.as<uint32_t>(), cols, d.csize.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    k_dedup_ids<<<g, 256, 0, st>>>(zf, d.rep.as<uint32_t>(), d.csize.as<uint32_t>(), cols, d.cid.as<uint32_t>(),
+                                   d.values.as<Fr>(), d.nclass.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    k_dedup_mark<<<g, 256, 0, st>>>(d.rep.as<uint32_t>(), d.cid.as<uint32_t>(), cols,
+                                    d.class_of.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int msm_class_sort_alloc(MsmClassSort &s, uint64_t n)
+{
+    s.n = n;
+    NKR_TRY(s.counts.alloc((kClassMax + 1) * 4ull, "class counts"));
+    NKR_TRY(s.offsets.alloc((kClassMax + 1) * 4ull, "class offsets"));
+    NKR_TRY(s.cursor.alloc((kClassMax + 1) * 4ull, "class cursor"));
+    NKR_TRY(s.entries.alloc(std::max<uint64_t>(n, 1) * 4, "class members"));
+    NKR_TRY(s.scan_tmp.alloc(scan_scratch_words(kClassMax) * 4, "class scan scratch"));
+    return NKR_B200_OK;
+}
+
+int msm_class_sort_run(MsmClassSort &s, const MsmDedup &d, const uint32_t *gather, cudaStream_t st)
+{
+    NKR_CUDA(cudaMemsetAsync(s.counts.p, 0, (kClassMax + 1) * 4ull, st));
+    if (s.n)
+        k_cls_count<<<blocks_for(s.n, 256), 256, 0, st>>>(d.class_of.as<uint32_t>(), gather, s.n,
+                                                            s.counts.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    NKR_TRY(scan_exclusive(LoadU32{s.counts.as<uint32_t>()}, kClassMax, s.offsets.as<uint32_t>(),
+                           s.scan_tmp.as<uint32_t>(), st));
+    NKR_CUDA(cudaMemcpyAsync(s.cursor.p, s.offsets.p, kClassMax * 4ull, cudaMemcpyDeviceToDevice, st));
+    if (s.n)
+        k_cls_scatter<<<blocks_for(s.n, 256), 256, 0, st>>>(d.class_of.as<uint32_t>(), gather, s.n,
+                                                              s.cursor.as<uint32_t>(), s.entries.as<uint32_t>());
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int msm_class_acc_alloc(MsmClassAcc &a, int group, uint64_t n)
+{
+    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
+    NKR_TRY(group == 1 ? class_acc_alloc_t<Fq>(a, n) : class_acc_alloc_t<Fq2>(a, n));
+    a.small.group = group;
+    a.small.shape = msm_shape(kClassMax, false, group);
+    NKR_TRY(a.small.pts.alloc(uint64_t(kClassMax) * (group == 1 ? sizeof(G1Affine) : sizeof(G2Affine)),
+                              "class sums (affine)"));
+    // the MSM over the class values ends with a Horner chain of ~250 doublings;
+    // G2 runs its reduction levels on lane pairs (half the chain's latency)
+    a.small_s.acc.lane_pairs = group == 2;
+    NKR_TRY(msm_scratch_alloc(a.small_s, group, a.small.shape));
+    NKR_TRY(a.out.alloc(group == 1 ? 96 : 192, "class MSM result"));
+    return NKR_B200_OK;
+}
+
+int msm_class_acc_issue(const MsmBases &b, const MsmClassSort &cs, const MsmDedup &d, MsmClassAcc &a,
+                        cudaStream_t st)
+{
+    NKR_REQUIRE(b.group == a.small.group, "class path and bases of different groups");
+    NKR_REQUIRE(cs.n == a.seg.n, "class sort and class sums of different supports");
+    NKR_TRY(b.group == 1 ? class_acc_issue_t<Fq>(b, cs, a, st) : class_acc_issue_t<Fq2>(b, cs, a, st));
+    return msm_run(a.small, a.small_s, d.values.p, a.out.p, st);
+}
+
+int msm_result_add(int group, void *out_dev, const void *add_dev, cudaStream_t st)
+{
+    NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
+    if (group == 1)
+        k_result_add<Fq><<<1, 32, 0, st>>>(static_cast<Fq *>(out_dev), static_cast<const Fq *>(add_dev));
+    else
+        k_result_add<Fq2><<<1, 32, 0, st>>>(static_cast<Fq2 *>(out_dev), static_cast<const Fq2 *>(add_dev));
+    NKR_CHECK_LAUNCH();
+    return NKR_B200_OK;
+}
+
+int msm_class_acc_run(const MsmBases &b, const MsmClassSort &cs, const MsmDedup &d, MsmClassAcc &a,
+                      void *out_dev, cudaStream_t st)
+{
+    NKR_TRY(msm_class_acc_issue(b, cs, d, a, st));
+    return msm_result_add(b.group, out_dev, a.out.p, st);
 }
 
 } // namespace nkr

@@ -145,9 +145,11 @@ int msm_acc_alloc(MsmAcc &a, int group, const MsmShape &shape);
 int msm_scratch_alloc(MsmScratch &s, int group, const MsmShape &shape);
 
 // Sort the scalars Fr[n] (Montgomery, device) for the shape.
-// scalar i of the sort is scalars_dev[gather ? gather[i] : i]
+// scalar i of the sort is scalars_dev[gather ? gather[i] : i]; with class_of, a
+// scalar whose variable belongs to a class (class_of[v] != kNoClass, MsmDedup
+// below) counts as zero (the class path adds it)
 int msm_sort_run(const MsmShape &shape, MsmSort &s, const void *scalars_dev, cudaStream_t st,
-                 const uint32_t *gather = nullptr);
+                 const uint32_t *gather = nullptr, const uint32_t *class_of = nullptr);
 // Accumulate / reduce with a finished sort of the same shape.  The result is
 // written to out_dev in libff Jacobian layout with an arbitrary Z (or Z = 0 for
 // infinity); normalise on the host (host/fr_host.hpp normalize_g1 / _g2).
@@ -171,5 +173,80 @@ int msm_acc_level1_list(int group, const MsmAccJob *jobs, int n, void *items_hos
 int msm_acc_tail(const MsmBases &b, const MsmSort &s, MsmAcc &a, void *out_dev, cudaStream_t st);
 // the level-1 kernel of msm_acc_run alone (msm_acc_tail finishes the MSM)
 int msm_acc_level1(const MsmBases &b, const MsmSort &s, MsmAcc &a, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Repeated scalars.  A witness repeats values (constant wires, the same wire of
+// every copy of a gadget: the 2^20-constraint Poseidon benchmark holds 899 K
+// nonzero values of which 169 K are distinct, 829 values covering 731 K
+// variables).  With classes c of variables of equal value v_c,
+//     sum_i w_i P_i = sum_{i in no class} w_i P_i + sum_c v_c S_c,
+//     S_c = sum_{i in c} P_i,
+// so a class member costs one point addition into S_c instead of W entries of
+// the digit sort; a small MSM over the classes adds the second sum.  The split is
+// exact for any partition into classes of equal values, so a witness without
+// repetition only pays the class-finding pass.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kNoClass = 0xffffffffu;
+constexpr uint32_t kClassMax = 4096; // classes per prove; further repeated values stay singletons
+constexpr uint32_t kClassMin = 4;    // members of the smallest class (a class costs W' small-MSM entries)
+
+// Classes of one witness (per prove slot).  A hash table of variable indices
+// (linear probing on a hash of the value, full-value comparison) gives every
+// nonzero value a representative; representatives with at least kClassMin
+// members take class ids.
+struct MsmDedup {
+    DevBuf table, rep, csize, cid, class_of, values, nclass;
+    uint64_t cols = 0, slots = 0;
+    size_t device_bytes() const
+    {
+        return table.bytes + rep.bytes + csize.bytes + cid.bytes + class_of.bytes + values.bytes +
+               nclass.bytes;
+    }
+};
+int msm_dedup_alloc(MsmDedup &d, uint64_t cols);
+// z: Fr[cols] (Montgomery, device).  Afterwards class_of[v] is variable v's class
+// (kNoClass for zeros and singletons) and values[c] the value of class c (zero
+// for unused ids).
+int msm_dedup_run(MsmDedup &d, const void *z, cudaStream_t st);
+
+// The class members of one support (n points, gather as for msm_sort_run) in
+// class order: offsets[c] .. offsets[c + 1] index entries, which hold point
+// indices.
+struct MsmClassSort {
+    DevBuf counts, offsets, cursor, entries, scan_tmp;
+    uint64_t n = 0;
+    size_t device_bytes() const
+    {
+        return counts.bytes + offsets.bytes + cursor.bytes + entries.bytes + scan_tmp.bytes;
+    }
+};
+int msm_class_sort_alloc(MsmClassSort &s, uint64_t n);
+int msm_class_sort_run(MsmClassSort &s, const MsmDedup &d, const uint32_t *gather, cudaStream_t st);
+
+// One MSM's class path: the class sums S_c (summed like buckets: fixed segments,
+// fix-up levels), normalised to affine as the bases of a small MSM over the
+// class values.
+struct MsmClassAcc {
+    MsmShape seg;      // n = the support's points, nb = kClassMax classes, k1, k2
+    DevBuf partials, buckets, lead_off, scan_tmp;
+    MsmBases small;    // the class sums (affine), non-folded
+    MsmScratch small_s;
+    DevBuf out;        // sum_c v_c S_c, libff Jacobian layout
+    size_t device_bytes() const
+    {
+        return partials.bytes + buckets.bytes + lead_off.bytes + scan_tmp.bytes + small.device_bytes() +
+               small_s.device_bytes() + out.bytes;
+    }
+};
+int msm_class_acc_alloc(MsmClassAcc &a, int group, uint64_t n);
+// Class sums over bases b (its first n points: 2^0 window copies), the MSM over
+// the classes, and out_dev (the MSM's result, libff Jacobian) += that sum.
+int msm_class_acc_run(const MsmBases &b, const MsmClassSort &cs, const MsmDedup &d, MsmClassAcc &a,
+                      void *out_dev, cudaStream_t st);
+// the class-path part of msm_class_acc_run without the final addition (a.out
+// holds sum_c v_c S_c), and the addition alone
+int msm_class_acc_issue(const MsmBases &b, const MsmClassSort &cs, const MsmDedup &d, MsmClassAcc &a,
+                        cudaStream_t st);
+int msm_result_add(int group, void *out_dev, const void *add_dev, cudaStream_t st);
 
 } // namespace nkr

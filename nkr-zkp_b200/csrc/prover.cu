@@ -68,15 +68,19 @@ ProveSlot::~ProveSlot()
     if (graph) cudaGraphDestroy(graph);
     for (auto s : tail)
         if (s) cudaStreamSynchronize(s);
+    for (auto s : cls)
+        if (s) cudaStreamSynchronize(s);
     if (chain) cudaStreamSynchronize(chain);
     for (int k = 0; k < kNumMsm; ++k) {
         if (st[k]) cudaStreamDestroy(st[k]);
         if (tail[k]) cudaStreamDestroy(tail[k]);
+        if (cls[k]) cudaStreamDestroy(cls[k]);
         if (ev_done[k]) cudaEventDestroy(ev_done[k]);
         if (ev_l1[k]) cudaEventDestroy(ev_l1[k]);
+        if (ev_cls[k]) cudaEventDestroy(ev_cls[k]);
     }
     if (chain) cudaStreamDestroy(chain);
-    for (cudaEvent_t e : {ev_z, ev_wit[0], ev_wit[1], ev_hsorted})
+    for (cudaEvent_t e : {ev_z, ev_wit[0], ev_wit[1], ev_hsorted, ev_dedup})
         if (e) cudaEventDestroy(e);
     for (auto e : ev_sorted)
         if (e) cudaEventDestroy(e);
@@ -127,14 +131,23 @@ int slot_add(nkr_b200_key *key)
     // stream, in any order, with or without waiting for the quotient chain, took
     // 20.2-22.4 ms.
     const int prio = slot_stream_priority(key->logn);
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) cudaGetLastError();
+    const int cls_prio = prio - 2 < greatest ? greatest : prio - 2;
     for (int k = 0; k < kNumMsm; ++k) {
         NKR_CUDA(cudaStreamCreateWithPriority(&sl->st[k], cudaStreamNonBlocking, prio));
         NKR_CUDA(cudaStreamCreateWithPriority(&sl->tail[k], cudaStreamNonBlocking, prio));
+        // the class path is a chain of small, latency-bound launches: two priority
+        // levels above the slot's level-1 kernels, so its blocks do not queue
+        // behind theirs (cls[kMsmH] carries the class finding)
+        NKR_CUDA(cudaStreamCreateWithPriority(&sl->cls[k], cudaStreamNonBlocking, cls_prio));
+        NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_cls[k], cudaEventDisableTiming));
         NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_done[k], cudaEventDisableTiming));
         NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_l1[k], cudaEventDisableTiming));
     }
     NKR_CUDA(cudaStreamCreateWithPriority(&sl->chain, cudaStreamNonBlocking, prio));
     NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_hsorted, cudaEventDisableTiming));
+    NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_dedup, cudaEventDisableTiming));
     NKR_CUDA(cudaEventCreateWithFlags(&sl->ev_z, cudaEventDisableTiming));
     for (auto &e : sl->ev_sorted) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : sl->ev_wit) NKR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -149,6 +162,19 @@ int slot_add(nkr_b200_key *key)
     }
     NKR_TRY(msm_sort_alloc(sl->sort_h, key->bases[kMsmH].shape));
     bytes += sl->sort_h.device_bytes();
+    NKR_TRY(msm_dedup_alloc(sl->dedup, key->cols));
+    bytes += sl->dedup.device_bytes();
+    for (int g = 0; g < key->n_sorts; ++g) {
+        const int o = key->sort_stream[g];
+        if (!key->classes[o]) continue;
+        NKR_TRY(msm_class_sort_alloc(sl->csort[g], key->bases[o].shape.n));
+        bytes += sl->csort[g].device_bytes();
+    }
+    for (int k = 0; k < kNumMsm; ++k) {
+        if (!key->classes[k]) continue;
+        NKR_TRY(msm_class_acc_alloc(sl->cacc[k], key->bases[k].group, key->bases[k].shape.n));
+        bytes += sl->cacc[k].device_bytes();
+    }
     for (int k = 0; k < kNumMsm; ++k) {
         // The G1 witness MSMs' reductions run beside other MSMs' level-1 work, so
         // their first level takes twice the buckets per thread (less work, more
@@ -203,18 +229,39 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
     if (timed) NKR_CUDA(cudaEventRecord(sl->ev_t[1], s0));
     // witness MSMs on their own streams, overlapping the H chain; one digit sort
     // of z (gathered through the bases' support) per distinct support
+    // classes of repeated witness values (main stream), then the digit sorts
+    // without the class members and the class members of each support
+    NKR_CUDA(cudaStreamWaitEvent(sl->cls[kMsmH], sl->ev_z, 0));
+    NKR_TRY(msm_dedup_run(sl->dedup, z, sl->cls[kMsmH]));
+    NKR_CUDA(cudaEventRecord(sl->ev_dedup, sl->cls[kMsmH]));
     for (int g = 0; g < key->n_sorts; ++g) {
         const int o = key->sort_stream[g];
-        NKR_CUDA(cudaStreamWaitEvent(sl->st[o], sl->ev_z, 0));
-        NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], z, sl->st[o], key->bases[o].gather()));
+        const bool cls = key->classes[o];
+        NKR_CUDA(cudaStreamWaitEvent(sl->st[o], cls ? sl->ev_dedup : sl->ev_z, 0));
+        NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], z, sl->st[o], key->bases[o].gather(),
+                             cls ? sl->dedup.class_of.as<uint32_t>() : nullptr));
+        if (cls) NKR_TRY(msm_class_sort_run(sl->csort[g], sl->dedup, key->bases[o].gather(), sl->st[o]));
         NKR_CUDA(cudaEventRecord(sl->ev_sorted[g], sl->st[o]));
     }
-    // level 1 on the MSM's stream, the fix-up and reduction levels on its tail stream
+    // level 1 on the MSM's stream, the fix-up and reduction levels on its tail
+    // stream; a class-path MSM runs its class sums and the MSM over the classes on
+    // its class stream (once its sort is done), beside its level 1 and tail, and
+    // its tail ends with the addition of the two results
     auto msm_issue = [&](int k, const MsmSort &so, cudaStream_t s_l1) -> int {
+        if (key->classes[k]) {
+            const int g = key->sort_of[k];
+            NKR_CUDA(cudaStreamWaitEvent(sl->cls[k], sl->ev_sorted[g], 0));
+            NKR_TRY(msm_class_acc_issue(key->bases[k], sl->csort[g], sl->dedup, sl->cacc[k], sl->cls[k]));
+            NKR_CUDA(cudaEventRecord(sl->ev_cls[k], sl->cls[k]));
+        }
         NKR_TRY(msm_acc_level1(key->bases[k], so, sl->acc[k], s_l1));
         NKR_CUDA(cudaEventRecord(sl->ev_l1[k], s_l1));
         NKR_CUDA(cudaStreamWaitEvent(sl->tail[k], sl->ev_l1[k], 0));
         NKR_TRY(msm_acc_tail(key->bases[k], so, sl->acc[k], out + kOutOffset[k], sl->tail[k]));
+        if (key->classes[k]) {
+            NKR_CUDA(cudaStreamWaitEvent(sl->tail[k], sl->ev_cls[k], 0));
+            NKR_TRY(msm_result_add(key->bases[k].group, out + kOutOffset[k], sl->cacc[k].out.p, sl->tail[k]));
+        }
         if (timed) NKR_CUDA(cudaEventRecord(sl->ev_msm_end[k], sl->tail[k]));
         NKR_CUDA(cudaEventRecord(sl->ev_done[k], sl->tail[k]));
         return NKR_B200_OK;
@@ -263,6 +310,7 @@ int slot_capture(nkr_b200_key *key, ProveSlot *sl)
     NKR_CUDA(cudaSetDevice(key->ctx->device));
     for (auto s : sl->st) NKR_CUDA(cudaStreamSynchronize(s));
     for (auto s : sl->tail) NKR_CUDA(cudaStreamSynchronize(s));
+    for (auto s : sl->cls) NKR_CUDA(cudaStreamSynchronize(s));
     NKR_CUDA(cudaStreamSynchronize(sl->chain));
     cudaStream_t s0 = sl->main();
     const unsigned long long before = g_kernel_launches.load();
@@ -385,13 +433,17 @@ int key_prepare(nkr_b200_ctx *ctx, const nkr_b200_circuit *c, const nkr_b200_pro
     int ch = 0;
     NKR_PREP(tuned_window_bits(ctx, c->rows, &ch));
     NKR_PREP(msm_bases_build(key->bases[kMsmH], 1, pk->h_query, false, c->rows, true, ch, true, st));
-    // MSMs with the same support (and so the same window shape) share a digit sort
+    // MSMs with the same support (and so the same window shape) and the same use
+    // of the class path share a digit sort
+    for (int k : kWitnessOrder) key->classes[k] = true;
     key->n_sorts = 0;
     for (int k : kWitnessOrder) {
         int g = -1;
         for (int h = 0; h < key->n_sorts && g < 0; ++h) {
-            const MsmBases &o = key->bases[key->sort_stream[h]];
-            if (o.shape.same_sort(key->bases[k].shape) && o.support_host == key->bases[k].support_host)
+            const int ho = key->sort_stream[h];
+            const MsmBases &o = key->bases[ho];
+            if (o.shape.same_sort(key->bases[k].shape) && o.support_host == key->bases[k].support_host &&
+                key->classes[ho] == key->classes[k])
                 g = h;
         }
         if (g < 0) {

@@ -54,6 +54,13 @@ struct ProveSlot {
     MsmSort sort_w[4]; // witness digit sorts, one per distinct support
     MsmSort sort_h;    // digit sort of H
     MsmAcc acc[kNumMsm];
+    // repeated witness values (msm.cuh): the witness's classes, the class members
+    // of each sort's support, and each class-path MSM's class sums and small MSM
+    MsmDedup dedup;
+    MsmClassSort csort[4];
+    MsmClassAcc cacc[kNumMsm];
+    cudaStream_t cls[kNumMsm] = {}; // class-path streams (class sums, MSM over the classes)
+    cudaEvent_t ev_dedup = nullptr, ev_cls[kNumMsm] = {};
     DevBuf z, az, bz, cz, h;
     DevBuf spmv_prod[3]; // SpMV products of the non-unit terms, per matrix
     DevBuf out; // 4 G1 + 1 G2 results, libff Jacobian layout (kOutBytes)
@@ -94,6 +101,9 @@ struct nkr_b200_key {
     int n_sorts = 0;
     int sort_of[nkr::kNumMsm] = {};
     int sort_stream[4] = {};
+    // the witness MSMs take repeated witness values through the class path (their
+    // sorts leave class members out)
+    bool classes[nkr::kNumMsm] = {};
     nkr::DevBuf pk_const; // alpha_g1, beta_g1, delta_g1 (G1 affine) and beta_g2, delta_g2 (G2 affine)
     nkr::DevBuf blind_io;  // raw proof and scalars in, proof out (blind.cu)
     nkr::DevBuf blind_tab; // fixed-base tables of alpha1, beta1, delta1 (G1) and delta2 (G2)

@@ -171,3 +171,49 @@ def test_prepare_rejects_bad_shapes(ctx):
     with pytest.raises(nk.B200Error):
         be.prove(r1.witness[:-1])
     be.free()
+
+
+def test_prove_repeated_witness_values(ctx, ref, tmp_path):
+    """Repeated witness values go through the class path of the G1 witness MSMs:
+    variables of equal value form a class whose bases are summed once, and a small
+    MSM over the class values adds v_c S_c.  A crafted witness with more
+    minimum-size classes (4 members) than one prove takes (4,096; the others stay
+    singletons), groups below the minimum, large classes (fix-up levels), values
+    beside their negations and zeros gives the reference CPU prover's raw proof,
+    before and after a prove of the circuit's own witness on the same slot."""
+    r1 = nk.generate("matmul", 32, 0, seed=31)
+    pk_path, vk_path = tmp_path / "c.pk.bin", tmp_path / "c.vk.bin"
+    ref.cpu_setup(r1, pk_path, vk_path)
+    pk = O.read_proving_key(pk_path)
+    rng = np.random.default_rng(77)
+    n = r1.cols
+    w = O.random_fr(n, rng)
+    w[0] = O.fr_mont(1)
+    vals = O.random_fr(4400, rng)
+    pos = rng.permutation(np.arange(1, n))
+    k = 0
+
+    def put(v, m):
+        nonlocal k
+        w[pos[k:k + m]] = v
+        k += m
+
+    for j in range(4200):
+        put(vals[j], 4)
+    for j in range(4200, 4300):
+        put(vals[j], 3)
+    for j in range(4300, 4310):
+        put(vals[j], 500)
+    for j in range(4310, 4320):
+        put(vals[j], 8)
+        put(O.int_to_limbs((O.R - O.limbs_to_int(vals[j])) % O.R), 8)
+    w[pos[k:k + 2000]] = 0
+    be = nk.Backend(ctx)
+    be.prepare(r1, pk)
+    raw = be.prove(w)
+    g1, g2 = _raw_affine(raw)
+    rg1, rg2 = ref.cpu_prove(r1, pk_path, w)
+    assert np.array_equal(g1, rg1) and np.array_equal(g2, rg2)
+    be.prove(r1.witness)
+    assert bytes(be.prove(w)) == bytes(raw)
+    be.free()
