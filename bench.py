@@ -157,6 +157,27 @@ def _measured_peaks():
         return {}
 
 
+def _uniform_fr(n, rng):
+    """n uniform Fr values (4 x u64 each, < r, taken as Montgomery limbs)"""
+    import numpy as np
+    r_limbs = [0x43e1f593f0000001, 0x2833e84879b97091, 0xb85045b68181585d, 0x30644e72e131a029]
+    out = np.empty((n, 4), np.uint64)
+    filled = 0
+    while filled < n:
+        k = n - filled
+        cand = rng.integers(0, 2**64, size=(k, 4), dtype=np.uint64, endpoint=False)
+        cand[:, 3] &= np.uint64((1 << 62) - 1)
+        less = np.zeros(k, bool)
+        equal = np.ones(k, bool)
+        for i in range(3, -1, -1):
+            less |= equal & (cand[:, i] < np.uint64(r_limbs[i]))
+            equal &= cand[:, i] == np.uint64(r_limbs[i])
+        good = cand[less]
+        out[filled:filled + good.shape[0]] = good
+        filled += good.shape[0]
+    return out
+
+
 def _seeded_toxic(seed):
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -436,6 +457,21 @@ def run_b200(args):
     h2d = r1.cols * 32 + 576 + 240
     d2h = 576 + 384
 
+    # ---- the same circuit over a witness without repeated values ----------------
+    # The witness MSMs sum the bases of equal witness values once (the benchmark
+    # witness repeats 829 values over 731 K variables); proves over seeded uniform
+    # values (all distinct; not a satisfying witness, which a prove does not check)
+    # show the cost when nothing repeats.
+    rng = np.random.default_rng(1234 + rank)
+    uni = torch.from_numpy(_uniform_fr(r1.cols, rng).view(np.int64).reshape(-1)).to(f"cuda:{device}")
+    for _ in range(2):
+        be.prove(None, witness_ptr=uni.data_ptr())
+    uni_ms = []
+    for _ in range(5):
+        be.prove(None, witness_ptr=uni.data_ptr())
+        uni_ms.append(be.stage_times()["total_ms"])
+    del uni
+
     # ---- roofline of the dominant kernel (MSM bucket accumulation) ---------------
     peaks = _measured_peaks()
     # The product roof is the instruction-issue ceiling of the 52-bit-limb Fq product
@@ -532,6 +568,9 @@ def run_b200(args):
         "config": _config(kind, param, dens, r1.rows, r1.cols, world),
         "key_device_gib": round(key_gb, 2),
         "stages_ms_median": s_med,
+        "prove_ms_distinct_witness": {"value": round(statistics.median(uni_ms), 3),
+                                      "note": "median of 5 device-timed proves of the same circuit "
+                                              "over seeded uniform Fr values (no repeated values)"},
         "msm_timeline_ms_median": {"phases": ["l1_start", "l1_end", "fixup_end",
                                               "reduce_first_end", "end"], **timeline},
         "prepare_ms": {"first": round(prep_ms[0], 1),

@@ -1650,7 +1650,9 @@ int msm_class_acc_alloc(MsmClassAcc &a, int group, uint64_t n)
     NKR_REQUIRE(group == 1 || group == 2, "group must be 1 (G1) or 2 (G2)");
     NKR_TRY(group == 1 ? class_acc_alloc_t<Fq>(a, n) : class_acc_alloc_t<Fq2>(a, n));
     a.small.group = group;
-    a.small.shape = msm_shape(kClassMax, false, group);
+    // 10-bit windows: 26 of them, so the Horner chain that ends the MSM has 25
+    // additions between its ~250 doublings (37 for the cost model's 7-bit windows)
+    a.small.shape = msm_shape(kClassMax, false, group, 10);
     NKR_TRY(a.small.pts.alloc(uint64_t(kClassMax) * (group == 1 ? sizeof(G1Affine) : sizeof(G2Affine)),
                               "class sums (affine)"));
     // the MSM over the class values ends with a Horner chain of ~250 doublings;

@@ -164,14 +164,10 @@ int slot_add(nkr_b200_key *key)
     bytes += sl->sort_h.device_bytes();
     NKR_TRY(msm_dedup_alloc(sl->dedup, key->cols));
     bytes += sl->dedup.device_bytes();
-    for (int g = 0; g < key->n_sorts; ++g) {
-        const int o = key->sort_stream[g];
-        if (!key->classes[o]) continue;
-        NKR_TRY(msm_class_sort_alloc(sl->csort[g], key->bases[o].shape.n));
-        bytes += sl->csort[g].device_bytes();
-    }
     for (int k = 0; k < kNumMsm; ++k) {
         if (!key->classes[k]) continue;
+        NKR_TRY(msm_class_sort_alloc(sl->csort[k], key->bases[k].shape.n));
+        bytes += sl->csort[k].device_bytes();
         NKR_TRY(msm_class_acc_alloc(sl->cacc[k], key->bases[k].group, key->bases[k].shape.n));
         bytes += sl->cacc[k].device_bytes();
     }
@@ -240,18 +236,17 @@ int prove_issue(nkr_b200_key *key, ProveSlot *sl, bool timed, bool blind_tables)
         NKR_CUDA(cudaStreamWaitEvent(sl->st[o], cls ? sl->ev_dedup : sl->ev_z, 0));
         NKR_TRY(msm_sort_run(key->bases[o].shape, sl->sort_w[g], z, sl->st[o], key->bases[o].gather(),
                              cls ? sl->dedup.class_of.as<uint32_t>() : nullptr));
-        if (cls) NKR_TRY(msm_class_sort_run(sl->csort[g], sl->dedup, key->bases[o].gather(), sl->st[o]));
         NKR_CUDA(cudaEventRecord(sl->ev_sorted[g], sl->st[o]));
     }
     // level 1 on the MSM's stream, the fix-up and reduction levels on its tail
     // stream; a class-path MSM runs its class sums and the MSM over the classes on
-    // its class stream (once its sort is done), beside its level 1 and tail, and
+    // its class stream (once the classes are known), beside its level 1 and tail, and
     // its tail ends with the addition of the two results
     auto msm_issue = [&](int k, const MsmSort &so, cudaStream_t s_l1) -> int {
         if (key->classes[k]) {
-            const int g = key->sort_of[k];
-            NKR_CUDA(cudaStreamWaitEvent(sl->cls[k], sl->ev_sorted[g], 0));
-            NKR_TRY(msm_class_acc_issue(key->bases[k], sl->csort[g], sl->dedup, sl->cacc[k], sl->cls[k]));
+            NKR_CUDA(cudaStreamWaitEvent(sl->cls[k], sl->ev_dedup, 0));
+            NKR_TRY(msm_class_sort_run(sl->csort[k], sl->dedup, key->bases[k].gather(), sl->cls[k]));
+            NKR_TRY(msm_class_acc_issue(key->bases[k], sl->csort[k], sl->dedup, sl->cacc[k], sl->cls[k]));
             NKR_CUDA(cudaEventRecord(sl->ev_cls[k], sl->cls[k]));
         }
         NKR_TRY(msm_acc_level1(key->bases[k], so, sl->acc[k], s_l1));

@@ -54,10 +54,10 @@ struct ProveSlot {
     MsmSort sort_w[4]; // witness digit sorts, one per distinct support
     MsmSort sort_h;    // digit sort of H
     MsmAcc acc[kNumMsm];
-    // repeated witness values (msm.cuh): the witness's classes, the class members
-    // of each sort's support, and each class-path MSM's class sums and small MSM
+    // repeated witness values (msm.cuh): the witness's classes, and each
+    // class-path MSM's class members, class sums and small MSM
     MsmDedup dedup;
-    MsmClassSort csort[4];
+    MsmClassSort csort[kNumMsm];
     MsmClassAcc cacc[kNumMsm];
     cudaStream_t cls[kNumMsm] = {}; // class-path streams (class sums, MSM over the classes)
     cudaEvent_t ev_dedup = nullptr, ev_cls[kNumMsm] = {};
