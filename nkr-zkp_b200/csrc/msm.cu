@@ -11,6 +11,7 @@
 
 #include "field52.cuh"
 #include "msm.cuh"
+#include "pairing.cuh" // twist_frobenius: the endomorphism psi of G2
 #include "scan.cuh"
 
 namespace nkr {
@@ -1318,6 +1319,55 @@ __global__ void k_result_add(F *acc, const F *add)
     acc[2] = s.zz * s.zzz;
 }
 
+// G2's MSM over its class values uses the twist Frobenius psi(x, y) =
+// (conj(x) gx1, conj(y) gy1), which acts on G2 as multiplication by
+// lambda = p mod r = 6 u^2 (127 bits): a class value v = k0 + k1 lambda with
+// k0 = v mod lambda and k1 = v div lambda (both below 2^128), so the MSM runs over
+// the class sums and their images under psi with 128-bit scalars, and its Horner
+// chain has half the doublings.
+constexpr uint64_t kPsiLambdaLo = 0xf83e9682e87cfd46ull, kPsiLambdaHi = 0x6f4d8248eeb859fbull;
+constexpr int kPsiWindows = 13; // 10-bit signed windows over 128-bit scalars (130 bits, no carry out)
+
+__device__ __forceinline__ Fr fr_from_u128(unsigned __int128 x)
+{
+    Fr r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r.v[i] = uint32_t(x >> (32 * i));
+#pragma unroll
+    for (int i = 4; i < 8; ++i) r.v[i] = 0;
+    return to_mont(r);
+}
+
+// values[c] (Montgomery) -> out[c] = k0, out[n + c] = k1 (Montgomery), by binary
+// long division of the canonical value by lambda
+__global__ void k_cls_split_psi(const Fr *__restrict__ values, uint32_t n, Fr *__restrict__ out)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const Fr v = from_mont(values[c]);
+    const unsigned __int128 lam = (unsigned __int128)kPsiLambdaHi << 64 | kPsiLambdaLo;
+    unsigned __int128 rem = 0, q = 0;
+    for (int i = 253; i >= 0; --i) { // v < r < 2^254; rem < lambda, so 2 rem + 1 < 2^128
+        rem = (rem << 1) | ((v.v[i >> 5] >> (i & 31)) & 1u);
+        q <<= 1;
+        if (rem >= lam) {
+            rem -= lam;
+            q |= 1;
+        }
+    }
+    out[c] = fr_from_u128(rem);
+    out[n + c] = fr_from_u128(q);
+}
+
+// sums[n + c] = psi(sums[c]) (infinity stays infinity)
+__global__ void k_cls_psi(Affine<Fq2> *sums, uint32_t n)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const Affine<Fq2> a = sums[c];
+    sums[n + c] = a.is_inf() ? a : twist_frobenius(a);
+}
+
 template <class F>
 int class_acc_alloc_t(MsmClassAcc &a, uint64_t n)
 {
@@ -1651,10 +1701,16 @@ int msm_class_acc_alloc(MsmClassAcc &a, int group, uint64_t n)
     NKR_TRY(group == 1 ? class_acc_alloc_t<Fq>(a, n) : class_acc_alloc_t<Fq2>(a, n));
     a.small.group = group;
     // 10-bit windows: 26 of them, so the Horner chain that ends the MSM has 25
-    // additions between its ~250 doublings (37 for the cost model's 7-bit windows)
-    a.small.shape = msm_shape(kClassMax, false, group, 10);
-    NKR_TRY(a.small.pts.alloc(uint64_t(kClassMax) * (group == 1 ? sizeof(G1Affine) : sizeof(G2Affine)),
-                              "class sums (affine)"));
+    // additions between its ~250 doublings (37 for the cost model's 7-bit windows);
+    // G2: the class sums and their psi images with 128-bit scalars, 13 windows
+    const uint64_t pts = group == 1 ? kClassMax : 2ull * kClassMax;
+    a.small.shape = msm_shape(pts, false, group, 10);
+    if (group == 2) {
+        a.small.shape.W = kPsiWindows;
+        a.small.shape.nb = a.small.shape.B * uint32_t(kPsiWindows);
+        NKR_TRY(a.split.alloc(pts * sizeof(Fr), "class value halves"));
+    }
+    NKR_TRY(a.small.pts.alloc(pts * (group == 1 ? sizeof(G1Affine) : sizeof(G2Affine)), "class sums (affine)"));
     // the MSM over the class values ends with a Horner chain of ~250 doublings;
     // G2 runs its reduction levels on lane pairs (half the chain's latency)
     a.small_s.acc.lane_pairs = group == 2;
@@ -1669,7 +1725,13 @@ int msm_class_acc_issue(const MsmBases &b, const MsmClassSort &cs, const MsmDedu
     NKR_REQUIRE(b.group == a.small.group, "class path and bases of different groups");
     NKR_REQUIRE(cs.n == a.seg.n, "class sort and class sums of different supports");
     NKR_TRY(b.group == 1 ? class_acc_issue_t<Fq>(b, cs, a, st) : class_acc_issue_t<Fq2>(b, cs, a, st));
-    return msm_run(a.small, a.small_s, d.values.p, a.out.p, st);
+    if (b.group == 1) return msm_run(a.small, a.small_s, d.values.p, a.out.p, st);
+    const unsigned g = blocks_for(kClassMax, 128);
+    k_cls_psi<<<g, 128, 0, st>>>(a.small.pts.as<Affine<Fq2>>(), kClassMax);
+    NKR_CHECK_LAUNCH();
+    k_cls_split_psi<<<g, 128, 0, st>>>(d.values.as<Fr>(), kClassMax, a.split.as<Fr>());
+    NKR_CHECK_LAUNCH();
+    return msm_run(a.small, a.small_s, a.split.p, a.out.p, st);
 }
 
 int msm_result_add(int group, void *out_dev, const void *add_dev, cudaStream_t st)

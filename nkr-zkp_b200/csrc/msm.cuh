@@ -229,13 +229,14 @@ int msm_class_sort_run(MsmClassSort &s, const MsmDedup &d, const uint32_t *gathe
 struct MsmClassAcc {
     MsmShape seg;      // n = the support's points, nb = kClassMax classes, k1, k2
     DevBuf partials, buckets, lead_off, scan_tmp;
-    MsmBases small;    // the class sums (affine), non-folded
+    MsmBases small;    // the class sums (affine; G2: and their psi images), non-folded
     MsmScratch small_s;
+    DevBuf split;      // G2: the class values as k0 + k1 lambda (msm.cu)
     DevBuf out;        // sum_c v_c S_c, libff Jacobian layout
     size_t device_bytes() const
     {
         return partials.bytes + buckets.bytes + lead_off.bytes + scan_tmp.bytes + small.device_bytes() +
-               small_s.device_bytes() + out.bytes;
+               small_s.device_bytes() + split.bytes + out.bytes;
     }
 };
 int msm_class_acc_alloc(MsmClassAcc &a, int group, uint64_t n);
