@@ -118,3 +118,18 @@ def test_reference_accepts_generated_witness(ref):
         bad = r.witness.copy()
         bad[1] = O.fr_mont(O.fr_int(bad[1]) + 1)
         assert not ref.check_witness(r, bad)
+
+
+def test_benchmark_witness_repeats_values():
+    """The 2^20-constraint benchmark witness (poseidon count 2048, sparse) repeats
+    values: 899,483 nonzero of 1,048,576 variables take 169,390 distinct values
+    (one of them zero), 829 of which cover 880,015 variables.  The witness MSMs'
+    class path sums the bases of each repeated value once, so the prove time of the
+    benchmark depends on this (bench.py also reports a prove over distinct values)."""
+    r1 = nk.generate("poseidon", 2048, 2, seed=1)
+    w = np.ascontiguousarray(np.asarray(r1.witness)).view(np.uint8).reshape(-1, 32)
+    vals, counts = np.unique(w, axis=0, return_counts=True)
+    assert w.shape[0] == 1 << 20
+    assert int(w.any(axis=1).sum()) == 899483
+    assert vals.shape[0] == 169390
+    assert int((counts >= 2).sum()) == 829 and int(counts[counts >= 2].sum()) == 880015
