@@ -13,7 +13,9 @@
 // Streams of a slot: after the witness upload and the SpMV, the four witness
 // MSMs (a, b_g1, l on G1 and b_g2 on G2) run on their own streams while the
 // main stream computes H (7 transforms) and then the H MSM; the reference runs
-// every stage serially with a device sync after each.
+// every stage serially with a device sync after each.  The witness's repeated
+// values are found once per prove, and each witness MSM sums the bases of every
+// class of equal values on a class stream of higher priority (msm.cuh).
 #pragma once
 
 #include <cstdint>
