@@ -503,7 +503,8 @@ def run_b200(args):
         # DRAM bytes per entry from an ncu capture of this kernel at 2^18, scaled to
         # this launch's entries
         traffic = round(st["entries"] * TRAFFIC_PER_ENTRY) if TRAFFIC_PER_ENTRY else None
-        roof = {"bound": "int", "kernel": "k_acc_l1_g1 (G1 bucket accumulation)",
+        roof = {"bound": "int", "kernel": "k_acc_l1_g1 (G1 bucket accumulation; operator-level MSM "
+                                          "over the A query and the workload's witness, no class path)",
                 "achieved": round(achieved / 1e9, 2), "peak": round(issue_peak / 1e9, 2),
                 "unit": "G Fq-mul/s", "frac": round(achieved / issue_peak, 3),
                 "peak_source": f"instruction-issue ceiling of the FP64-limb Fq product: {sms} SMs "
